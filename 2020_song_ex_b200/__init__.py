@@ -1,0 +1,293 @@
+"""song_b200 -- B200-native SONG graph search behind the reference's interface.
+
+Python mirror of the reference's search entry points (lrlorry/2020_song_ex),
+calling the sm_100a kernels through the C ABI of ``include/song_b200.h``
+(``libsong_b200.so``, built in-tree by ``build.py``):
+
+* :class:`Params`           -- config.h:9-58 as runtime values.
+* :class:`KernelGraph`      -- kernalGraph.h:20-71 (data + adj; ``upload_to_gpu``).
+* :class:`HashKernelGraph`  -- hashKernelGraph.h:22-126 (codes + adj).
+* :func:`gpu_search`        -- kernalGraph.h:307-382 and the Hamming overload
+  hashKernelGraph.h:360-435: returns the flat ``[nq*k]`` id list, best-first,
+  ``-1`` padded, optionally filling a :class:`GpuSearchTrace`.
+* :func:`search_device`     -- the same search on device-resident tensors.
+
+There is no CPU fallback: if the library is missing or no GPU is present the
+calls raise :class:`SongError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field, fields
+from typing import List, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsong_b200.so")
+
+SONG_OK = 0
+SONG_ERR_INVALID_ARG = 1
+SONG_ERR_OOM = 2
+SONG_ERR_CUDA = 3
+SONG_ERR_TIMEOUT = 4
+SONG_ERR_BUDGET = 5
+SONG_ERR_UNSUPPORTED = 6
+KIND_L2 = 0
+KIND_HAMMING = 1
+
+TRACE_FIELDS = (
+    "seed_count", "visited_nodes", "expanded_nodes", "neighbor_slots_scanned",
+    "candidate_nodes", "distance_evals", "frontier_pushes", "result_updates",
+    "peak_frontier", "peak_results", "result_count", "early_stopped",
+)
+
+
+class SongError(RuntimeError):
+    """A song_b200 call failed; ``status`` is the song_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[song status {status}] {message}")
+        self.status = status
+
+
+class _Params(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "block_size", "fixed_degree", "search_degree", "ef_construction", "pq_size", "topk",
+        "n_multiprobe", "n_multiquery", "hash_bits", "bf_words", "bf_nhash")]
+
+
+class _Timing(C.Structure):
+    _fields_ = [("alloc_ms", C.c_double), ("h2d_ms", C.c_double), ("memset_ms", C.c_double),
+                ("kernel_ms", C.c_double), ("d2h_ms", C.c_double), ("total_ms", C.c_double),
+                ("ef_search", C.c_int), ("batch_limit", C.c_int), ("n_batches", C.c_int)]
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def load_library(build_if_missing: bool = True) -> C.CDLL:
+    """Load libsong_b200.so (building it first when absent and nvcc is present)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise SongError(SONG_ERR_UNSUPPORTED, f"{LIB_PATH} is missing; run build.py")
+        from importlib import import_module
+        import_module(__name__ + ".build").build()
+    L = C.CDLL(LIB_PATH)
+    vp, i64, ci = C.c_void_p, C.c_int64, C.c_int
+    L.song_params_default.argtypes = [C.POINTER(_Params)]
+    L.song_params_default.restype = None
+    L.song_last_error.restype = C.c_char_p
+    L.song_version.restype = C.c_char_p
+    L.song_index_create_l2.argtypes = [vp, i64, ci, vp, C.POINTER(_Params), C.POINTER(vp)]
+    L.song_index_create_hamming.argtypes = [vp, i64, ci, vp, C.POINTER(_Params), C.POINTER(vp)]
+    L.song_index_destroy.argtypes = [vp]
+    L.song_index_info.argtypes = [vp, C.POINTER(i64), C.POINTER(ci), C.POINTER(ci)]
+    L.song_gpu_search.argtypes = [vp, vp, ci, ci, ci, ci, vp, vp, C.POINTER(_Timing)]
+    L.song_gpu_search_hamming.argtypes = [vp, vp, ci, ci, ci, ci, vp, vp, C.POINTER(_Timing)]
+    L.song_search_device.argtypes = [vp, vp, ci, ci, ci, vp, vp, vp]
+    L.song_kernel_launch_count.restype = C.c_int64
+    for name in ("song_index_create_l2", "song_index_create_hamming", "song_index_destroy",
+                 "song_index_info", "song_gpu_search", "song_gpu_search_hamming",
+                 "song_search_device"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != SONG_OK:
+        msg = load_library().song_last_error().decode(errors="replace")
+        raise SongError(status, msg)
+
+
+def launch_count() -> int:
+    """Search-kernel launches issued by the library in this process."""
+    return int(load_library().song_kernel_launch_count())
+
+
+@dataclass
+class Params:
+    """config.h:9-58 as runtime values; defaults are the reference's."""
+    block_size: int = 32       # BLOCK_SIZE
+    fixed_degree: int = 31     # FIXED_DEGREE
+    search_degree: int = 15    # SEARCH_DEGREE
+    ef_construction: int = 150 # EF_CONSTRUCTION
+    pq_size: int = 50          # pq_size
+    topk: int = 10             # TOPK
+    n_multiprobe: int = 4      # N_MULTIPROBE
+    n_multiquery: int = 512    # N_MULTIQUERY
+    hash_bits: int = 256       # hash_bits
+    bf_words: int = 256        # BF_WORDS
+    bf_nhash: int = 4          # BF_NHASH
+
+    @property
+    def hash_words(self) -> int:  # HASH_WORDS, config.h:44
+        return self.hash_bits // 32
+
+    def _c(self) -> _Params:
+        return _Params(**{f.name: int(getattr(self, f.name)) for f in fields(self)})
+
+
+@dataclass
+class QueryTrace:
+    """telemetry.h:5-18."""
+    seed_count: int = 0
+    visited_nodes: int = 0
+    expanded_nodes: int = 0
+    neighbor_slots_scanned: int = 0
+    candidate_nodes: int = 0
+    distance_evals: int = 0
+    frontier_pushes: int = 0
+    result_updates: int = 0
+    peak_frontier: int = 0
+    peak_results: int = 0
+    result_count: int = 0
+    early_stopped: int = 0
+
+
+@dataclass
+class GpuSearchTrace:
+    """telemetry.h:30-41; ``queries`` is an int32 array [nq, 12] in QueryTrace order."""
+    ef_search: int = 0
+    batch_limit: int = 0
+    alloc_ms: float = 0.0
+    h2d_ms: float = 0.0
+    memset_ms: float = 0.0
+    kernel_ms: float = 0.0
+    d2h_ms: float = 0.0
+    total_ms: float = 0.0
+    n_batches: int = 0
+    queries: np.ndarray = field(default_factory=lambda: np.zeros((0, 12), np.int32))
+
+    def query(self, i: int) -> QueryTrace:
+        return QueryTrace(*(int(v) for v in self.queries[i]))
+
+
+class _Index:
+    kind = KIND_L2
+
+    def __init__(self, params: Optional[Params]):
+        self.params = params or Params()
+        self._h = C.c_void_p()
+
+    @property
+    def uploaded(self) -> bool:
+        return bool(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            load_library().song_index_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class KernelGraph(_Index):
+    """kernalGraph.h:20-71: FP32 ``data [n, dim]`` + ``adj [n, block_size]``."""
+    kind = KIND_L2
+
+    def __init__(self, num_nodes: int, dim: int, data, params: Optional[Params] = None,
+                 adj=None):
+        super().__init__(params)
+        self.num_nodes = int(num_nodes)
+        self.dim = int(dim)
+        self.data = np.ascontiguousarray(np.asarray(data, dtype=np.float32).reshape(num_nodes, dim))
+        bs = self.params.block_size
+        self.adj = (np.full((num_nodes, bs), -1, np.int32) if adj is None
+                    else np.ascontiguousarray(np.asarray(adj, dtype=np.int32).reshape(num_nodes, bs)))
+
+    def add_vertex(self, u: int, neighbors) -> None:
+        """kernalGraph.h:32-35."""
+        m = min(len(neighbors), self.params.fixed_degree)
+        self.adj[u, :m] = np.asarray(neighbors[:m], dtype=np.int32)
+
+    def upload_to_gpu(self) -> None:
+        """kernalGraph.h:38-43 (replaces any earlier upload)."""
+        self.close()
+        L = load_library()
+        _check(L.song_index_create_l2(self.data.ctypes.data, self.num_nodes, self.dim,
+                                      self.adj.ctypes.data, C.byref(self.params._c()),
+                                      C.byref(self._h)))
+
+
+class HashKernelGraph(_Index):
+    """hashKernelGraph.h:22-126: packed ``hashed [n, hash_words]`` codes + ``adj``."""
+    kind = KIND_HAMMING
+
+    def __init__(self, num_nodes: int, hashed, params: Optional[Params] = None, adj=None):
+        super().__init__(params)
+        self.num_nodes = int(num_nodes)
+        self.hashed = np.ascontiguousarray(np.asarray(hashed, dtype=np.uint32).reshape(num_nodes, -1))
+        self.hash_words = self.hashed.shape[1]
+        bs = self.params.block_size
+        self.adj = (np.full((num_nodes, bs), -1, np.int32) if adj is None
+                    else np.ascontiguousarray(np.asarray(adj, dtype=np.int32).reshape(num_nodes, bs)))
+
+    def upload_to_gpu(self) -> None:
+        self.close()
+        L = load_library()
+        _check(L.song_index_create_hamming(self.hashed.ctypes.data, self.num_nodes,
+                                           self.hash_words, self.adj.ctypes.data,
+                                           C.byref(self.params._c()), C.byref(self._h)))
+
+
+def gpu_search(g, queries, nq: int, k: int, N_MULTIQUERY: int = 512, ef_search: Optional[int] = None,
+               trace: Optional[GpuSearchTrace] = None) -> np.ndarray:
+    """gpu_search (kernalGraph.h:307-382 / hashKernelGraph.h:360-435).
+
+    ``queries`` is ``[nq, dim]`` FP32 for a :class:`KernelGraph` or
+    ``[nq, hash_words]`` uint32 codes for a :class:`HashKernelGraph`.
+    ``ef_search`` defaults to ``pq_size`` and is clamped like the reference.
+    Returns the flat ``[nq*k]`` int32 ids, best-first, -1 padded.
+    """
+    if not g.uploaded:
+        raise SongError(SONG_ERR_INVALID_ARG, "graph not uploaded (call upload_to_gpu first)")
+    L = load_library()
+    ef = g.params.pq_size if ef_search is None else int(ef_search)
+    if g.kind == KIND_L2:
+        q = np.ascontiguousarray(np.asarray(queries, dtype=np.float32).reshape(nq, g.dim))
+        fn = L.song_gpu_search
+    else:
+        q = np.ascontiguousarray(np.asarray(queries, dtype=np.uint32).reshape(nq, g.hash_words))
+        fn = L.song_gpu_search_hamming
+    ids = np.empty(max(nq * k, 1), dtype=np.int32)
+    tq = np.zeros((nq, 12), dtype=np.int32) if trace is not None else None
+    t = _Timing()
+    _check(fn(g._h, q.ctypes.data, nq, k, N_MULTIQUERY, ef, ids.ctypes.data,
+              tq.ctypes.data if tq is not None else None, C.byref(t)))
+    if trace is not None:
+        trace.ef_search, trace.batch_limit = t.ef_search, t.batch_limit
+        trace.alloc_ms, trace.h2d_ms, trace.memset_ms = t.alloc_ms, t.h2d_ms, t.memset_ms
+        trace.kernel_ms, trace.d2h_ms, trace.total_ms = t.kernel_ms, t.d2h_ms, t.total_ms
+        trace.n_batches = t.n_batches
+        trace.queries = tq
+    return ids[: nq * k]
+
+
+def search_device(g, d_queries, nq: int, k: int, ef_search: int, d_ids, d_traces=None,
+                  stream=None) -> None:
+    """Asynchronous search on device pointers (ints) or torch CUDA tensors."""
+    def ptr(x):
+        if x is None:
+            return None
+        return int(x.data_ptr()) if hasattr(x, "data_ptr") else int(x)
+    st = None
+    if stream is not None:
+        st = int(getattr(stream, "cuda_stream", stream))
+    _check(load_library().song_search_device(g._h, ptr(d_queries), nq, k, ef_search, ptr(d_ids),
+                                             ptr(d_traces), st))

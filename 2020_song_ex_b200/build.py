@@ -1,0 +1,60 @@
+"""Build the sm_100a shared library ``libsong_b200.so`` in-tree with nvcc.
+
+Usage: ``python 2020_song_ex_b200/build.py [--verbose]``.  The library is
+written next to this file so that it travels with the source tree.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libsong_b200.so")
+SOURCES = ["song_search.cu", "song_capi.cu"]
+NVCC = os.environ.get("NVCC", "nvcc")
+FLAGS = [
+    "-std=c++17", "-O3", "-lineinfo",
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-Xcompiler", "-fPIC",
+    "--expt-relaxed-constexpr",
+]
+
+
+def sources() -> list[str]:
+    return [os.path.join(CSRC, s) for s in SOURCES]
+
+
+def _deps() -> list[str]:
+    out = sources()
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        out += [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".h", ".cuh", ".hpp"))]
+    return out
+
+
+def stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(p) > t for p in _deps())
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not stale():
+        return LIB
+    tmp = LIB + ".tmp"
+    cmd = [NVCC, *FLAGS, "-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+           *sources(), "-o", tmp]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose="--verbose" in sys.argv)
+    print(LIB)

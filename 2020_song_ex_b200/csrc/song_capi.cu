@@ -1,0 +1,393 @@
+// song_capi.cu -- the C ABI of include/song_b200.h.
+//
+// Replaces the reference's host layer: KernelGraph / HashKernelGraph with
+// upload_to_gpu (kernalGraph.h:20-71, hashKernelGraph.h:22-126) and
+// gpu_search (kernalGraph.h:307-382, hashKernelGraph.h:360-435).
+// Differences that do not change results:
+//  * the index owns its device buffers for its lifetime (the reference
+//    cudaMallocs and frees query/result buffers on every call, :326-330);
+//  * every CUDA call is checked and reported as a song_status;
+//  * a host-pointer search stages queries in chunks of
+//    max(n_multiquery, 16384) and runs each chunk as ONE persistent launch
+//    (results do not depend on batching: queries are independent).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "song_b200.h"
+#include "song_kernels.cuh"
+
+namespace song {
+extern std::atomic<int64_t> g_launches;
+}
+
+struct song_index {
+    int kind = SONG_KIND_L2;
+    int64_t n = 0;
+    int dim = 0;  // floats (L2) or u32 words (Hamming) per vector
+    int ld = 0;   // padded row stride in elements (multiple of 4)
+    song_params p{};
+    int device = 0;
+    int num_sms = 0;
+    void* d_base = nullptr;
+    int32_t* d_adj = nullptr;
+    unsigned* d_counter = nullptr;  // ring of work counters, one per launch (kCounterRing)
+    unsigned counter_next = 0;
+    int* d_err = nullptr;
+    // staging buffers of the host-pointer entry points, grown on demand
+    void* d_q = nullptr;
+    size_t q_cap = 0;
+    int32_t* d_ids = nullptr;
+    size_t ids_cap = 0;
+    song_query_trace* d_tr = nullptr;
+    size_t tr_cap = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+song_status fail(song_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+song_status cuda_fail(cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(e == cudaErrorMemoryAllocation ? SONG_ERR_OOM : SONG_ERR_CUDA, m);
+}
+
+#define SONG_CUDA(call, what)                              \
+    do {                                                   \
+        cudaError_t _e = (call);                           \
+        if (_e != cudaSuccess) return cuda_fail(_e, what); \
+    } while (0)
+
+int round_up4(int x) { return (x + 3) / 4 * 4; }
+
+// Each launch takes the next work counter of a ring, so launches that
+// overlap on different streams do not share one; a counter is reused after
+// kCounterRing launches on the same index.
+constexpr unsigned kCounterRing = 1024;
+
+song_status check_params(const song_params* p) {
+    if (p == nullptr) return fail(SONG_ERR_INVALID_ARG, "params is NULL");
+    if (p->block_size < 1) return fail(SONG_ERR_INVALID_ARG, "block_size must be >= 1");
+    if (p->pq_size < 1) return fail(SONG_ERR_INVALID_ARG, "pq_size must be >= 1");
+    if (p->n_multiprobe < 1) return fail(SONG_ERR_INVALID_ARG, "n_multiprobe must be >= 1");
+    if (p->bf_words < 1) return fail(SONG_ERR_INVALID_ARG, "bf_words must be >= 1");
+    if (p->bf_nhash < 1 || p->bf_nhash > 4)
+        return fail(SONG_ERR_UNSUPPORTED, "bf_nhash must be 1..4 (the reference table holds 4 hashes)");
+    if ((int64_t)p->bf_words * 64 > (int64_t)INT32_MAX)
+        return fail(SONG_ERR_UNSUPPORTED, "bf_words too large");
+    return SONG_OK;
+}
+
+song_status check_adj(const int32_t* adj, int64_t n, int bs) {
+    const int64_t total = n * (int64_t)bs;
+    for (int64_t i = 0; i < total; ++i) {
+        const int32_t v = adj[i];
+        if (v >= n || v < -1) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "adj[%lld] = %d is neither -1 nor a node id in [0, %lld)",
+                          (long long)i, v, (long long)n);
+            return fail(SONG_ERR_INVALID_ARG, buf);
+        }
+    }
+    return SONG_OK;
+}
+
+void free_index(song_index* x) {
+    if (x == nullptr) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(x->device);
+    cudaFree(x->d_base);
+    cudaFree(x->d_adj);
+    cudaFree(x->d_counter);
+    cudaFree(x->d_err);
+    cudaFree(x->d_q);
+    cudaFree(x->d_ids);
+    cudaFree(x->d_tr);
+    if (x->ev0) cudaEventDestroy(x->ev0);
+    if (x->ev1) cudaEventDestroy(x->ev1);
+    if (x->stream) cudaStreamDestroy(x->stream);
+    cudaSetDevice(cur);
+    delete x;
+}
+
+// Upload rows of `dim` elements (4 bytes each) into a padded [n x ld] buffer.
+song_status create_common(int kind, const void* rows, int64_t n, int dim, const int32_t* adj,
+                          const song_params* params, song_index** out) {
+    if (out == nullptr) return fail(SONG_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (song_status s = check_params(params)) return s;
+    if (rows == nullptr || adj == nullptr) return fail(SONG_ERR_INVALID_ARG, "data or adj is NULL");
+    if (n < 1 || n > (int64_t)INT32_MAX) return fail(SONG_ERR_INVALID_ARG, "n must be in [1, 2^31)");
+    if (dim < 1) return fail(SONG_ERR_INVALID_ARG, "dim must be >= 1");
+    if (kind == SONG_KIND_HAMMING && dim > 32)
+        return fail(SONG_ERR_UNSUPPORTED, "hash_words must be <= 32 (1024-bit codes)");
+    if (song_status s = check_adj(adj, n, params->block_size)) return s;
+
+    song_index* x = new (std::nothrow) song_index();
+    if (x == nullptr) return fail(SONG_ERR_OOM, "host allocation failed");
+    x->kind = kind;
+    x->n = n;
+    x->dim = dim;
+    x->ld = round_up4(dim);
+    x->p = *params;
+    cudaError_t e = cudaGetDevice(&x->device);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, x->device);
+    const size_t row_bytes = (size_t)x->ld * 4;
+    if (e == cudaSuccess) e = cudaMalloc(&x->d_base, (size_t)n * row_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&x->d_adj, (size_t)n * params->block_size * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&x->d_counter, kCounterRing * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&x->d_err, 256);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&x->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&x->ev1);
+    if (e == cudaSuccess && x->ld != dim) e = cudaMemset(x->d_base, 0, (size_t)n * row_bytes);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2D(x->d_base, row_bytes, rows, (size_t)dim * 4, (size_t)dim * 4, (size_t)n,
+                         cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(x->d_adj, adj, (size_t)n * params->block_size * sizeof(int32_t),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(x->d_err, 0, 256);
+    if (e != cudaSuccess) {
+        song_status s = cuda_fail(e, "index upload");
+        free_index(x);
+        return s;
+    }
+    *out = x;
+    return SONG_OK;
+}
+
+template <typename T>
+cudaError_t grow(T** ptr, size_t* cap, size_t bytes) {
+    if (*cap >= bytes) return cudaSuccess;
+    cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc((void**)ptr, bytes);
+    if (e == cudaSuccess) *cap = bytes;
+    return e;
+}
+
+int clamp_ef(int ef, int k, int pq_size) {  // kernalGraph.h:315-316
+    if (ef < k) ef = k;
+    if (ef > pq_size) ef = pq_size;
+    return ef;
+}
+
+// Fill SearchArgs for one launch over `nq` queries at d_q / d_ids / d_tr.
+song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int32_t* d_ids,
+                      song_query_trace* d_tr, song::SearchArgs* a) {
+    const int cap = ef < 1 ? 1 : (ef > x->p.pq_size ? x->p.pq_size : ef);  // Candidates::init
+    std::memset(a, 0, sizeof *a);
+    a->base = x->d_base;
+    a->adj = x->d_adj;
+    a->queries = d_q;
+    a->out = d_ids;
+    a->trace = d_tr;
+    a->counter = x->d_counter;
+    a->err = x->d_err;
+    a->n = x->n;
+    a->dim = x->dim;
+    a->ld = x->ld;
+    a->qld = x->dim;
+    a->block_size = x->p.block_size;
+    a->k = k;
+    a->nq = nq;
+    a->cap = cap;
+    a->bf_words = x->p.bf_words;
+    a->bf_nhash = x->p.bf_nhash;
+    a->n_multiprobe = x->p.n_multiprobe;
+    song::search_warp_smem(x->kind, x->dim, cap, x->p.bf_words, a);
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, x->device);
+    if (a->warp_smem > optin) {
+        char buf[200];
+        std::snprintf(buf, sizeof buf,
+                      "per-query shared memory %d B (queue %d, bf_words %d, dim %d) exceeds the "
+                      "%d B a CTA may use",
+                      a->warp_smem, cap, x->p.bf_words, x->dim, optin);
+        return fail(SONG_ERR_UNSUPPORTED, buf);
+    }
+    return SONG_OK;
+}
+
+song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
+    unsigned* ctr = x->d_counter + (x->counter_next++ % kCounterRing);
+    a.counter = ctr;
+    SONG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), st), "counter reset");
+    cudaError_t e = song::launch_search(x->kind, a, x->num_sms, st);
+    if (e != cudaSuccess) return cuda_fail(e, "search launch");
+    return SONG_OK;
+}
+
+song_status host_search(song_index* x, int kind, const void* queries, int nq, int k,
+                        int n_multiquery, int ef_search, int32_t* ids, song_query_trace* traces,
+                        song_timing* timing) {
+    using clk = std::chrono::high_resolution_clock;
+    auto ms = [](clk::time_point a, clk::time_point b) {
+        return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (x->kind != kind) return fail(SONG_ERR_INVALID_ARG, "query type does not match the index kind");
+    if (nq < 0 || k < 0) return fail(SONG_ERR_INVALID_ARG, "nq and k must be >= 0");
+    if (nq > 0 && (queries == nullptr || (k > 0 && ids == nullptr)))
+        return fail(SONG_ERR_INVALID_ARG, "queries or ids is NULL");
+    const int ef = clamp_ef(ef_search, k, x->p.pq_size);
+    song_timing t{};
+    t.ef_search = ef;
+    t.batch_limit = n_multiquery;
+    std::lock_guard<std::mutex> lock(x->mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != x->device) SONG_CUDA(cudaSetDevice(x->device), "cudaSetDevice");
+    const int chunk = std::max(std::max(n_multiquery, 1), std::min(nq, 16384));
+    const size_t qrow = (size_t)x->dim * 4;
+    auto t0 = clk::now();
+    SONG_CUDA(grow(&x->d_q, &x->q_cap, std::max<size_t>(1, (size_t)std::min(nq, chunk) * qrow)),
+              "query staging alloc");
+    SONG_CUDA(grow(&x->d_ids, &x->ids_cap, std::max<size_t>(4, (size_t)std::min(nq, chunk) * k * 4)),
+              "result staging alloc");
+    if (traces)
+        SONG_CUDA(grow(&x->d_tr, &x->tr_cap,
+                       std::max<size_t>(48, (size_t)std::min(nq, chunk) * sizeof(song_query_trace))),
+                  "trace staging alloc");
+    auto t1 = clk::now();
+    t.alloc_ms = ms(t0, t1);
+    cudaStream_t st = x->stream;
+    for (int off = 0; off < nq; off += chunk) {
+        const int bs = std::min(chunk, nq - off);
+        auto b0 = clk::now();
+        SONG_CUDA(cudaMemcpyAsync(x->d_q, (const char*)queries + (size_t)off * qrow, (size_t)bs * qrow,
+                                  cudaMemcpyHostToDevice, st),
+                  "query H2D");
+        SONG_CUDA(cudaStreamSynchronize(st), "query H2D sync");
+        auto b1 = clk::now();
+        song::SearchArgs a;
+        if (song_status s = make_args(x, x->d_q, bs, k, ef, x->d_ids, traces ? x->d_tr : nullptr, &a))
+            return s;
+        SONG_CUDA(cudaEventRecord(x->ev0, st), "event");
+        if (song_status s = launch(x, a, st)) return s;
+        SONG_CUDA(cudaEventRecord(x->ev1, st), "event");
+        SONG_CUDA(cudaStreamSynchronize(st), "search kernel");
+        float kms = 0.f;
+        cudaEventElapsedTime(&kms, x->ev0, x->ev1);
+        auto b2 = clk::now();
+        if (k > 0)
+            SONG_CUDA(cudaMemcpyAsync(ids + (size_t)off * k, x->d_ids, (size_t)bs * k * 4,
+                                      cudaMemcpyDeviceToHost, st),
+                      "ids D2H");
+        if (traces)
+            SONG_CUDA(cudaMemcpyAsync(traces + off, x->d_tr, (size_t)bs * sizeof(song_query_trace),
+                                      cudaMemcpyDeviceToHost, st),
+                      "trace D2H");
+        SONG_CUDA(cudaStreamSynchronize(st), "D2H sync");
+        auto b3 = clk::now();
+        t.h2d_ms += ms(b0, b1);
+        t.kernel_ms += kms;
+        t.d2h_ms += ms(b2, b3);
+        t.n_batches += 1;
+    }
+    int err = 0;
+    SONG_CUDA(cudaMemcpy(&err, x->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+    if (err) return fail(SONG_ERR_INVALID_ARG, "graph holds an out-of-range neighbour id");
+    t.total_ms = ms(t1, clk::now());
+    if (timing) *timing = t;
+    return SONG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void song_params_default(song_params* p) {
+    if (!p) return;
+    p->block_size = 32;        // config.h:9
+    p->fixed_degree = 31;      // config.h:12
+    p->search_degree = 15;     // config.h:17
+    p->ef_construction = 150;  // config.h:24
+    p->pq_size = 50;           // config.h:28
+    p->topk = 10;              // config.h:31
+    p->n_multiprobe = 4;       // config.h:34
+    p->n_multiquery = 512;     // config.h:38
+    p->hash_bits = 256;        // config.h:41
+    p->bf_words = 256;         // config.h:56
+    p->bf_nhash = 4;           // config.h:58
+}
+
+const char* song_last_error(void) { return g_err.c_str(); }
+
+const char* song_version(void) { return "song_b200 0.1 (sm_100a)"; }
+
+song_status song_index_create_l2(const float* data, int64_t n, int dim, const int32_t* adj,
+                                 const song_params* params, song_index** out) {
+    return create_common(SONG_KIND_L2, data, n, dim, adj, params, out);
+}
+
+song_status song_index_create_hamming(const uint32_t* codes, int64_t n, int hash_words,
+                                      const int32_t* adj, const song_params* params,
+                                      song_index** out) {
+    return create_common(SONG_KIND_HAMMING, codes, n, hash_words, adj, params, out);
+}
+
+song_status song_index_destroy(song_index* index) {
+    free_index(index);
+    return SONG_OK;
+}
+
+song_status song_index_info(const song_index* x, int64_t* n, int* dim, int* kind) {
+    if (!x) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (n) *n = x->n;
+    if (dim) *dim = x->dim;
+    if (kind) *kind = x->kind;
+    return SONG_OK;
+}
+
+song_status song_gpu_search(song_index* index, const float* queries, int nq, int k,
+                            int n_multiquery, int ef_search, int32_t* ids,
+                            song_query_trace* traces, song_timing* timing) {
+    return host_search(index, SONG_KIND_L2, queries, nq, k, n_multiquery, ef_search, ids, traces,
+                       timing);
+}
+
+song_status song_gpu_search_hamming(song_index* index, const uint32_t* queries, int nq, int k,
+                                    int n_multiquery, int ef_search, int32_t* ids,
+                                    song_query_trace* traces, song_timing* timing) {
+    return host_search(index, SONG_KIND_HAMMING, queries, nq, k, n_multiquery, ef_search, ids,
+                       traces, timing);
+}
+
+song_status song_search_device(song_index* x, const void* d_queries, int nq, int k, int ef_search,
+                               int32_t* d_ids, song_query_trace* d_traces, void* stream) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (nq < 0 || k < 0) return fail(SONG_ERR_INVALID_ARG, "nq and k must be >= 0");
+    if (nq == 0) return SONG_OK;
+    if (d_queries == nullptr || (k > 0 && d_ids == nullptr))
+        return fail(SONG_ERR_INVALID_ARG, "queries or ids is NULL");
+    const int ef = clamp_ef(ef_search, k, x->p.pq_size);
+    std::lock_guard<std::mutex> lock(x->mu);
+    song::SearchArgs a;
+    if (song_status s = make_args(x, d_queries, nq, k, ef, d_ids, d_traces, &a)) return s;
+    return launch(x, a, (cudaStream_t)stream);
+}
+
+int64_t song_kernel_launch_count(void) { return song::g_launches.load(); }
+
+}  // extern "C"

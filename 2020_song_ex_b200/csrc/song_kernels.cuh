@@ -1,0 +1,41 @@
+// song_kernels.cuh -- launch interface of the sm_100a search kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "song_b200.h"
+
+namespace song {
+
+// Everything one search launch needs.  All pointers are device pointers.
+struct SearchArgs {
+    const void* base;        // FP32 [n x ld] (L2) or u32 [n x ld] (Hamming)
+    const int32_t* adj;      // [n x block_size], -1 = empty slot
+    const void* queries;     // [nq x qld], same element type as base
+    int32_t* out;            // [nq x k], best-first, -1 padded
+    song_query_trace* trace; // [nq] or nullptr
+    unsigned* counter;       // work counter: must be 0 at launch
+    int* err;                // set non-zero if an adjacency entry is out of range
+    int64_t n;
+    int dim;                 // elements compared per row (floats or u32 words)
+    int ld;                  // row stride of base, elements (multiple of 4)
+    int qld;                 // row stride of queries, elements
+    int block_size;          // BLOCK_SIZE
+    int k;
+    int nq;
+    int cap;                 // queue capacity = clamp(ef, 1, pq_size)
+    int bf_words;            // BF_WORDS
+    int bf_nhash;            // BF_NHASH (1..4)
+    int n_multiprobe;        // N_MULTIPROBE
+    int warp_smem;           // bytes of shared memory per warp (multiple of 16)
+    int q_off, cd_off, ci_off, rd_off, ri_off, bl_off;  // per-warp carve-up, bytes
+};
+
+// Per-warp shared-memory layout for (kind, dim, cap, bf_words).
+int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a);
+
+// Launch the plain search on `stream`: chooses the kernel instance for
+// (kind, dim), the warps per CTA and a persistent grid.  Returns a CUDA error.
+cudaError_t launch_search(int kind, const SearchArgs& a, int num_sms, cudaStream_t stream);
+
+}  // namespace song

@@ -1,0 +1,152 @@
+/*
+ * song_b200.h -- C ABI of the B200-native SONG graph search.
+ *
+ * Drop-in boundary for the reference's search path (lrlorry/2020_song_ex):
+ * plain pointers and sizes, no C++ or torch types.  Every entry point
+ * returns a song_status; song_last_error() gives the message of the last
+ * failure on the calling thread.  The reference checks no errors at all
+ * (its CUDA calls are unchecked, kernalGraph.h:39-45, :326-380).
+ *
+ * Semantics follow the reference GPU search exactly: for the same graph,
+ * queries and parameters the plain search returns the same top-k ids, in the
+ * same order including ties, and the same per-query QueryTrace counters as
+ * kg_search_kernel (kernalGraph.h:184-299) / hkg_search_kernel
+ * (hashKernelGraph.h:238-352).
+ */
+#ifndef SONG_B200_H
+#define SONG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int song_status;
+#define SONG_OK                0
+#define SONG_ERR_INVALID_ARG   1  /* bad size, pointer, parameter or graph entry   */
+#define SONG_ERR_OOM           2  /* device allocation failed                       */
+#define SONG_ERR_CUDA          3  /* a CUDA call failed (message has the reason)    */
+#define SONG_ERR_TIMEOUT       4  /* a bounded wait gave up                          */
+#define SONG_ERR_BUDGET        5  /* request exceeds a memory budget                 */
+#define SONG_ERR_UNSUPPORTED   6  /* parameters outside what the kernels implement   */
+
+/* Index kinds. */
+#define SONG_KIND_L2       0     /* FP32 vectors, squared L2 (kernalGraph.h)          */
+#define SONG_KIND_HAMMING  1     /* packed u32 sign codes, Hamming (hashKernelGraph.h) */
+
+/*
+ * Search/build parameters: the compile-time constants of config.h:9-58 as
+ * runtime values.  song_params_default() fills the reference defaults.
+ */
+typedef struct song_params {
+    int block_size;       /* BLOCK_SIZE      config.h:9   adjacency slots per node      */
+    int fixed_degree;     /* FIXED_DEGREE    config.h:12  (graph builder)               */
+    int search_degree;    /* SEARCH_DEGREE   config.h:17  (graph builder)               */
+    int ef_construction;  /* EF_CONSTRUCTION config.h:24  (graph builder)               */
+    int pq_size;          /* pq_size         config.h:28  queue capacity cap            */
+    int topk;             /* TOPK            config.h:31                                */
+    int n_multiprobe;     /* N_MULTIPROBE    config.h:34  entry points p*n/N            */
+    int n_multiquery;     /* N_MULTIQUERY    config.h:38  queries staged per batch      */
+    int hash_bits;        /* hash_bits       config.h:41  sign-projection code length   */
+    int bf_words;         /* BF_WORDS        config.h:56  Bloom filter 64-bit words     */
+    int bf_nhash;         /* BF_NHASH        config.h:58  Bloom hashes (1..4)           */
+} song_params;
+
+/* QueryTrace (telemetry.h:5-18): 12 int counters, same order and layout. */
+typedef struct song_query_trace {
+    int seed_count;
+    int visited_nodes;
+    int expanded_nodes;
+    int neighbor_slots_scanned;
+    int candidate_nodes;
+    int distance_evals;
+    int frontier_pushes;
+    int result_updates;
+    int peak_frontier;
+    int peak_results;
+    int result_count;
+    int early_stopped;
+} song_query_trace;
+
+/* The scalar part of GpuSearchTrace (telemetry.h:30-41). Times in ms. */
+typedef struct song_timing {
+    double alloc_ms;
+    double h2d_ms;
+    double memset_ms;
+    double kernel_ms;     /* CUDA-event time of the search kernels */
+    double d2h_ms;
+    double total_ms;
+    int ef_search;        /* ef after the reference clamp */
+    int batch_limit;      /* n_multiquery as passed */
+    int n_batches;
+} song_timing;
+
+typedef struct song_index song_index;
+
+/* Reference defaults of config.h:9-58. */
+void song_params_default(song_params* p);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* song_last_error(void);
+
+/* Library version string. */
+const char* song_version(void);
+
+/*
+ * Create an L2 index: uploads data[n x dim] (FP32, row-major) and
+ * adj[n x block_size] (int32, -1 = empty slot) to the current CUDA device.
+ * Replaces KernelGraph + upload_to_gpu (kernalGraph.h:20-43).  Every adj
+ * entry must be -1 or a node id in [0, n).
+ */
+song_status song_index_create_l2(const float* data, int64_t n, int dim, const int32_t* adj,
+                                 const song_params* params, song_index** out);
+
+/*
+ * Create a Hamming index over packed codes[n x hash_words] (u32).
+ * Replaces HashKernelGraph + upload_to_gpu (hashKernelGraph.h:22-98).
+ * hash_words must be a multiple of 4 and at most 32.
+ */
+song_status song_index_create_hamming(const uint32_t* codes, int64_t n, int hash_words,
+                                      const int32_t* adj, const song_params* params,
+                                      song_index** out);
+
+/* Frees the device copies (the KernelGraph destructor, kernalGraph.h:45). */
+song_status song_index_destroy(song_index* index);
+
+/* n, dim (floats or code words) and kind of an index. */
+song_status song_index_info(const song_index* index, int64_t* n, int* dim, int* kind);
+
+/*
+ * gpu_search (kernalGraph.h:307-382): host queries[nq x dim] in, host
+ * ids[nq x k] out (best-first, -1 padded).  ef_search is clamped exactly as
+ * the reference does (raise to k, then cap at pq_size).  traces (host,
+ * nq entries) and timing may be NULL.  Synchronous, like the reference.
+ */
+song_status song_gpu_search(song_index* index, const float* queries, int nq, int k,
+                            int n_multiquery, int ef_search, int32_t* ids,
+                            song_query_trace* traces, song_timing* timing);
+
+/* gpu_search overload of hashKernelGraph.h:360-435 on u32 query codes. */
+song_status song_gpu_search_hamming(song_index* index, const uint32_t* queries, int nq, int k,
+                                    int n_multiquery, int ef_search, int32_t* ids,
+                                    song_query_trace* traces, song_timing* timing);
+
+/*
+ * Device-resident search: d_queries (FP32 or u32 codes, by index kind),
+ * d_ids[nq x k] and d_traces (nullable) are device pointers; the call is
+ * asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * Same clamp and results as song_gpu_search.
+ */
+song_status song_search_device(song_index* index, const void* d_queries, int nq, int k,
+                               int ef_search, int32_t* d_ids, song_query_trace* d_traces,
+                               void* stream);
+
+/* Number of search-kernel launches issued by this library since load. */
+int64_t song_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SONG_B200_H */
