@@ -91,6 +91,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_gpu_search_hamming.argtypes = [vp, vp, ci, ci, ci, ci, vp, vp, C.POINTER(_Timing)]
     L.song_search_device.argtypes = [vp, vp, ci, ci, ci, vp, vp, vp]
     L.song_kernel_launch_count.restype = C.c_int64
+    L.song_build_graph.argtypes = [ci, vp, i64, ci, C.POINTER(_Params), ci, ci, vp]
+    L.song_build_graph.restype = C.c_int
     for name in ("song_index_create_l2", "song_index_create_hamming", "song_index_destroy",
                  "song_index_info", "song_gpu_search", "song_gpu_search_hamming",
                  "song_search_device"):
@@ -244,6 +246,34 @@ class HashKernelGraph(_Index):
         _check(L.song_index_create_hamming(self.hashed.ctypes.data, self.num_nodes,
                                            self.hash_words, self.adj.ctypes.data,
                                            C.byref(self.params._c()), C.byref(self._h)))
+
+
+def build_graph(rows, params: Optional[Params] = None, kind: int = KIND_L2,
+                batch_ratio: int = 32, build_bf_words: int = 1024) -> np.ndarray:
+    """NSW adjacency [n, block_size] built on the GPU (song_build_graph).
+
+    The reference's insertion algorithm (kernalGraph.h:140-149) run in
+    batches of max(1, inserted/batch_ratio) nodes; ``rows`` is FP32
+    ``[n, dim]`` for KIND_L2 or uint32 codes ``[n, words]`` for KIND_HAMMING.
+    """
+    params = params or Params()
+    dt = np.float32 if kind == KIND_L2 else np.uint32
+    rows = np.ascontiguousarray(np.asarray(rows, dtype=dt))
+    n, dim = rows.shape
+    adj = np.empty((n, params.block_size), dtype=np.int32)
+    _check(load_library().song_build_graph(kind, rows.ctypes.data, n, dim,
+                                           C.byref(params._c()), batch_ratio, build_bf_words,
+                                           adj.ctypes.data))
+    return adj
+
+
+def build_kernel_graph(data, n: int, dim: int, params: Optional[Params] = None,
+                       batch_ratio: int = 32) -> KernelGraph:
+    """build_kernel_graph (kernalGraph.h:140-149), built on the GPU."""
+    params = params or Params()
+    data = np.ascontiguousarray(np.asarray(data, dtype=np.float32).reshape(n, dim))
+    adj = build_graph(data, params, KIND_L2, batch_ratio)
+    return KernelGraph(n, dim, data, params, adj=adj)
 
 
 def gpu_search(g, queries, nq: int, k: int, N_MULTIQUERY: int = 512, ef_search: Optional[int] = None,

@@ -388,6 +388,47 @@ song_status song_search_device(song_index* x, const void* d_queries, int nq, int
     return launch(x, a, (cudaStream_t)stream);
 }
 
+song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
+                             const song_params* params, int batch_ratio, int build_bf_words,
+                             int32_t* adj_out) {
+    if (song_status s = check_params(params)) return s;
+    if (rows == nullptr || adj_out == nullptr) return fail(SONG_ERR_INVALID_ARG, "rows or adj_out is NULL");
+    if (kind != SONG_KIND_L2 && kind != SONG_KIND_HAMMING) return fail(SONG_ERR_INVALID_ARG, "bad kind");
+    if (n < 1 || n > (int64_t)INT32_MAX - 1) return fail(SONG_ERR_INVALID_ARG, "n must be in [1, 2^31-1)");
+    if (dim < 1 || (kind == SONG_KIND_HAMMING && dim > 32))
+        return fail(SONG_ERR_INVALID_ARG, "dim out of range");
+    if (params->fixed_degree < 1 || params->fixed_degree > 32 ||
+        params->fixed_degree > params->block_size || params->search_degree < 1 ||
+        params->ef_construction < 1)
+        return fail(SONG_ERR_UNSUPPORTED, "GPU build needs 1 <= fixed_degree <= min(32, block_size)");
+    const int bfw = build_bf_words > 0 ? build_bf_words : 1024;
+    const int ld = round_up4(dim);
+    int dev = 0, sms = 0;
+    SONG_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    SONG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    void* d_rows = nullptr;
+    int32_t* d_adj = nullptr;
+    cudaStream_t st = nullptr;
+    const size_t row_bytes = (size_t)ld * 4;
+    cudaError_t e = cudaMalloc(&d_rows, (size_t)n * row_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&d_adj, (size_t)n * params->block_size * 4);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess && ld != dim) e = cudaMemset(d_rows, 0, (size_t)n * row_bytes);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2D(d_rows, row_bytes, rows, (size_t)dim * 4, (size_t)dim * 4, (size_t)n,
+                         cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = song::build_graph_device(kind, d_rows, n, dim, ld, *params, batch_ratio, bfw, d_adj,
+                                     sms, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(adj_out, d_adj, (size_t)n * params->block_size * 4, cudaMemcpyDeviceToHost);
+    cudaFree(d_rows);
+    cudaFree(d_adj);
+    if (st) cudaStreamDestroy(st);
+    if (e != cudaSuccess) return cuda_fail(e, "graph build");
+    return SONG_OK;
+}
+
 int64_t song_kernel_launch_count(void) { return song::g_launches.load(); }
 
 }  // extern "C"

@@ -38,4 +38,9 @@ int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a);
 // (kind, dim), the warps per CTA and a persistent grid.  Returns a CUDA error.
 cudaError_t launch_search(int kind, const SearchArgs& a, int num_sms, cudaStream_t stream);
 
+// Batched-insertion NSW build over device rows (song_build.cu).
+cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim, int ld,
+                               const song_params& p, int ratio, int bf_words, int32_t* d_adj,
+                               int num_sms, cudaStream_t st);
+
 }  // namespace song

@@ -38,8 +38,12 @@ def _pick(rng: np.random.Generator, n: int, n_comp: int) -> np.ndarray:
 
 
 def int_mixture(n: int, nq: int, dim: int = 128, n_comp: int = 64, sigma: float = 20.0,
-                seed: int = 0, chunk: int = 1 << 18) -> Mixture:
-    """Integer-valued FP32 points: centre ~ U[0,255]^dim + N(0, sigma^2), clip, round."""
+                seed: int = 0, chunk: int = 1 << 18, query_seed=None) -> Mixture:
+    """Integer-valued FP32 points: centre ~ U[0,255]^dim + N(0, sigma^2), clip, round.
+
+    ``query_seed`` draws the queries from the same mixture with a separate
+    generator (independent query sets over one base, e.g. one per GPU).
+    """
     rng = np.random.default_rng(seed)
     centres = rng.uniform(0.0, 255.0, size=(n_comp, dim))
 
@@ -54,6 +58,8 @@ def int_mixture(n: int, nq: int, dim: int = 128, n_comp: int = 64, sigma: float 
         return out
 
     base = draw(n)
+    if query_seed is not None:
+        rng = np.random.default_rng(query_seed)
     queries = draw(nq)
     return Mixture(base, queries, seed)
 

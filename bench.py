@@ -1,0 +1,504 @@
+"""Benchmark: QPS at recall@10 >= 0.95 of the SONG graph search on B200.
+
+Workload (one "step" = one pass of the search over the whole query batch):
+1,000,000 x 128 integer-valued FP32 base vectors from a 1,024-component
+Gaussian mixture (centres U[0,255], sigma 20, clipped and rounded), 10,000
+queries from the same mixture, NSW graph with BLOCK_SIZE 32 (degree 31) built
+on the GPU, k = 10.  Synthetic, seeded stand-in for SIFT1M-shaped data (the
+public set is not available).  The queue size ef (and the Bloom filter size)
+is the smallest point of a sweep whose recall@10 against exact GPU
+brute-force ground truth reaches 0.95.
+
+Outputs one JSON line (rank 0).  ``value`` is device-resident QPS (queries
+and graph already in HBM); ``e2e`` is the same through the host C-ABI call
+(gpu_search with pinned host queries, H2D + kernel + D2H in the timed region).
+
+``--impl reference`` times the reference's own CPU search (Graph::search,
+graph.h:33-115, compiled from the reference sources into oracle/_ref) on the
+host cores, at the ef where IT reaches recall@10 0.95 on the same graph.
+
+Multi-GPU (torchrun): replicas only -- each rank searches its own 10,000
+queries on its own copy of the graph; no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BASE = 1_000_000
+DIM = 128
+N_COMP = 1024
+NQ = 10_000
+K = 10
+SEED = 2020
+BLOCK_SIZE = 32
+TARGET_RECALL = 0.95
+EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 512, 640, 768, 1024)
+BF_SWEEP = (256, 1024)
+WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self) -> dict:
+        if self.p is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(rank: int):
+    """Same base on every rank (replicas); rank r > 0 draws its own queries
+    from the same mixture."""
+    ds = importlib.import_module("2020_song_ex_b200.datasets")
+    m = ds.int_mixture(N_BASE, NQ, dim=DIM, n_comp=N_COMP, seed=SEED,
+                       query_seed=None if rank == 0 else SEED + 7919 * rank)
+    return m.base, m.queries
+
+
+def build_graph(song, base):
+    return song.build_graph(base, song.Params(block_size=BLOCK_SIZE, fixed_degree=BLOCK_SIZE - 1),
+                            batch_ratio=32)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the search kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+            return d.get("bytes_per_launch_scaled"), d.get("source")
+        except (OSError, ValueError):
+            pass
+    return None, None
+
+
+def bytes_per_query(trace: np.ndarray, k: int) -> np.ndarray:
+    """Algorithmic bytes: E*dim*4 + X*BLOCK_SIZE*4 + dim*4 + k*4 per query."""
+    E = trace[:, 5].astype(np.float64)
+    X = trace[:, 2].astype(np.float64)
+    return E * DIM * 4 + X * BLOCK_SIZE * 4 + DIM * 4 + k * 4
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import torch.distributed as dist
+    song = importlib.import_module("2020_song_ex_b200")
+    ds = importlib.import_module("2020_song_ex_b200.datasets")
+    gtm = importlib.import_module("2020_song_ex_b200.groundtruth")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    t0 = time.time()
+    base, queries = make_workload(rank)
+    adj = build_graph(song, base)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    gt, _ = gtm.knn(base, queries, K)
+    spot = gtm.spot_check(base, queries, gt, sample=16)
+    torch.cuda.empty_cache()
+    log(f"[rank {rank}] workload+graph {build_s:.1f}s, gt spot-check {spot}")
+
+    dq = torch.from_numpy(queries).to(dev)
+    d_ids = torch.empty((NQ, K), dtype=torch.int32, device=dev)
+    d_tr = torch.empty((NQ, 12), dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    # operating point: fastest (ef, bf_words) with recall@10 >= 0.95
+    curve, best = [], None
+    graphs = {}
+    sweep = BF_SWEEP if not args.ef else (args.bf_words,)
+    for bfw in sweep:
+        g = song.KernelGraph(N_BASE, DIM, base, song.Params(pq_size=1024, bf_words=bfw), adj=adj)
+        g.upload_to_gpu()
+        graphs[bfw] = g
+        for ef in (EF_SWEEP if not args.ef else (args.ef,)):
+            song.search_device(g, dq, NQ, K, ef, d_ids, d_tr, stream=stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream)
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1)
+            rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
+            pt = {"ef": ef, "bf_words": bfw, "recall": round(rec, 4), "qps": round(NQ / ms * 1e3)}
+            curve.append(pt)
+            if (rec >= TARGET_RECALL or args.ef) and (best is None or pt["qps"] > best["qps"]):
+                best = pt
+            if rec >= TARGET_RECALL:
+                break
+    if best is None:  # not reached: report the highest-recall point
+        best = max(curve, key=lambda p: (p["recall"], p["qps"]))
+    for bfw, g in graphs.items():
+        if bfw != best["bf_words"]:
+            g.close()
+    g = graphs[best["bf_words"]]
+    ef = best["ef"]
+    log(f"[rank {rank}] operating point {best}")
+
+    # traces of the operating point -> algorithmic bytes per launch
+    song.search_device(g, dq, NQ, K, ef, d_ids, d_tr, stream=stream)
+    stream.synchronize()
+    trace = d_tr.cpu().numpy()
+    ids_op = d_ids.cpu().numpy()
+    recall = float(ds.recall_at_k(ids_op, gt, K).mean())
+    launch_bytes = float(bytes_per_query(trace, K).sum())
+
+    # bit-exactness at full size on a sample of queries (oracle is the checker)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        import oracle
+        sample = 64
+        oids, otr = oracle.search_l2(base, adj, BLOCK_SIZE, queries[:sample], K, ef, pq_size=1024,
+                                     bf_words=best["bf_words"])
+        parity = bool((oids == ids_op[:sample]).all() and (otr == trace[:sample]).all())
+
+    # ---------------- timed region: device-resident
+    for _ in range(args.warmup):
+        song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream)
+    stream.synchronize()
+    n_launch0 = song.launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    gpu_index = local
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if cvd:
+        try:
+            gpu_index = int(cvd.split(",")[local])
+        except (ValueError, IndexError):
+            pass
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    with Clocks(gpu_index) as clk:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for i in range(args.steps):
+            evs[i][0].record(stream)
+            song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream)
+            evs[i][1].record(stream)
+        t_end.record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    if ws > 1:
+        dist.barrier()
+    launches = song.launch_count() - n_launch0
+    total_ms = t_start.elapsed_time(t_end)
+    kern_ms = [a.elapsed_time(b) for a, b in evs]
+    t = torch.tensor([total_ms], device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = ws * NQ * args.steps / (total_ms / 1e3)
+
+    # ---------------- e2e: host API, pinned host queries, H2D + kernel + D2H
+    if args.no_e2e:
+        g.close()
+        return {"value": round(value, 1), "note": "profiling case"} if rank == 0 else None
+    hq = torch.from_numpy(queries).pin_memory()
+    hids = torch.empty((NQ, K), dtype=torch.int32).pin_memory()
+    import ctypes as C
+    L = song.load_library()
+    timing = song._Timing()
+
+    def host_call():
+        st = L.song_gpu_search(g._h, C.c_void_p(hq.data_ptr()), NQ, K, NQ, ef,
+                               C.c_void_p(hids.data_ptr()), None, C.byref(timing))
+        if st != 0:
+            raise song.SongError(st, L.song_last_error().decode())
+
+    for _ in range(args.warmup):
+        host_call()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    h0 = time.perf_counter()
+    for _ in range(args.steps):
+        host_call()
+    e2e_s = time.perf_counter() - h0
+    te = torch.tensor([e2e_s], device=dev)
+    if ws > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_s = float(te.item())
+    assert np.array_equal(hids.numpy(), ids_op), "host-API ids differ from the device path"
+    e2e = {"value": round(ws * NQ * args.steps / e2e_s, 1), "unit": "queries/s",
+           "h2d_bytes_per_step": int(queries.nbytes), "d2h_bytes_per_step": int(NQ * K * 4)}
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = peaks()
+        avg_kern_s = statistics.mean(kern_ms) / 1e3
+        achieved = launch_bytes / avg_kern_s / 1e9
+        traffic, traffic_src = ncu_traffic()
+        cpu = None if args.no_cpu_baseline else cpu_baseline(base, adj, queries, gt, ef)
+        refgpu = None if args.no_ref_gpu else reference_gpu(base, adj, queries, gt, ef,
+                                                            best["bf_words"], ids_op)
+        out = {
+            "metric": "QPS at recall@10>=0.95 (plain bit-exact form)",
+            "value": round(value, 1),
+            "unit": "queries/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(total_ms / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)",
+            "config": {
+                "workload": WORKLOAD, "n": N_BASE, "dim": DIM, "nq_per_gpu": NQ, "k": K,
+                "ef": ef, "bf_words": best["bf_words"], "pq_size": 1024,
+                "graph": "GPU batched-insertion NSW (ratio 32)",
+                "l2": "inputs larger than L2 (data 512 MB + adj 128 MB per GPU)",
+                "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+            },
+            "recall_at_10": round(recall, 4),
+            "operating_point": best,
+            "recall_curve": curve,
+            "parity_sample_bit_exact": parity,
+            "gt_fp64_spot_check": {"queries": spot[0], "ids_missed": spot[1]},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "roofline": {
+                "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "traffic": traffic, "traffic_source": traffic_src,
+                "algorithmic_bytes_per_launch": round(launch_bytes),
+                "kernel_ms_avg": round(avg_kern_s * 1e3, 4),
+            },
+            "cpu_baseline": cpu,
+            "reference_gpu_kernel": refgpu,
+            "clocks": clk.summary(),
+            "trace_means": {k: round(float(v), 2) for k, v in
+                            zip(song.TRACE_FIELDS, trace.mean(axis=0))},
+            "build_s": round(build_s, 2),
+        }
+    g.close()
+    return out
+
+
+def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
+    """Reference CPU search (Graph::search) on a bounded sample, all host threads."""
+    try:
+        import oracle
+        r = oracle.ref(block_size=BLOCK_SIZE, bf_words=256, pq_size=512)
+    except Exception as e:  # reference not built
+        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                "sample": f"unavailable: {e}"}
+    ds = importlib.import_module("2020_song_ex_b200.datasets")
+    threads = os.cpu_count() or 1
+    cg = r.cpu_graph(base, adj)
+    cg.search(queries[:64], K, ef, threads=threads)  # warm
+    t0 = time.perf_counter()
+    ids, _ = cg.search(queries[:sample], K, ef, threads=threads)
+    dt = time.perf_counter() - t0
+    rec = float(ds.recall_at_k(ids, gt[:sample], K).mean())
+    cg.close()
+    return {"value": round(sample / dt, 1), "unit": "queries/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{sample} of the {NQ} queries at ef={ef}, Graph::search (graph.h:33) "
+                      f"from oracle/_ref on {threads} threads; its recall@10 {rec:.4f}"}
+
+
+def reference_gpu(base, adj, queries, gt, ef, bf_words, ours):
+    """The reference's own GPU kernel (kg_search_kernel via gpu_search, compiled
+    for sm_100a), same graph and parameters: QPS and id agreement."""
+    try:
+        import oracle
+        r = oracle.ref(block_size=BLOCK_SIZE, bf_words=bf_words, pq_size=1024)
+        if r.gpu is None:
+            raise FileNotFoundError("libref_gpu.so not built")
+    except Exception as e:
+        return {"unavailable": str(e)}
+    ids, _tr, timing = r.gpu_search_l2(base, adj, queries, K, ef)  # warm (JIT-free: sm_100a SASS)
+    ids, _tr, timing = r.gpu_search_l2(base, adj, queries, K, ef)
+    return {"qps_total": round(NQ / (timing[4] / 1e3), 1), "kernel_ms": round(timing[2], 3),
+            "total_ms": round(timing[4], 3), "ids_identical_to_ours": bool((ids == ours).all()),
+            "note": "gpu_search (kernalGraph.h:307) on the same graph: 512-query batches, H2D+kernel+D2H"}
+
+
+def run_reference(args, ws, rank, local):
+    """--impl reference: the reference CPU search on the host cores."""
+    if rank != 0:
+        return None
+    ds = importlib.import_module("2020_song_ex_b200.datasets")
+    try:
+        import oracle
+        r = oracle.ref(block_size=BLOCK_SIZE, bf_words=256, pq_size=512)
+    except Exception as e:
+        return {"impl": "reference", "unavailable": f"compiled reference not available: {e}"}
+    song = importlib.import_module("2020_song_ex_b200")
+    gtm = importlib.import_module("2020_song_ex_b200.groundtruth")
+    base, queries = make_workload(0)
+    adj = build_graph(song, base)  # setup only (same graph as our arm); untimed
+    gt, _ = gtm.knn(base, queries, K)
+    threads = os.cpu_count() or 1
+    cg = r.cpu_graph(base, adj)
+    rng = np.random.default_rng(1)
+    sweep_q = rng.choice(NQ, 400, replace=False)
+    ef_op, curve = None, []
+    for ef in EF_SWEEP:
+        ids, _ = cg.search(queries[sweep_q], K, ef, threads=threads)
+        rec = float(ds.recall_at_k(ids, gt[sweep_q], K).mean())
+        curve.append({"ef": ef, "recall": round(rec, 4)})
+        if rec >= TARGET_RECALL:
+            ef_op = ef
+            break
+    if ef_op is None:
+        ef_op = EF_SWEEP[-1]
+    per_step = args.ref_step_queries
+    times = []
+    for i in range(args.warmup + args.steps):
+        sel = np.arange(i * per_step, (i + 1) * per_step) % NQ
+        t0 = time.perf_counter()
+        cg.search(queries[sel], K, ef_op, threads=threads)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    total = sum(times)
+    qps = per_step * args.steps / total
+    ids, _ = cg.search(queries[:per_step], K, ef_op, threads=threads)
+    rec = float(ds.recall_at_k(ids, gt[:per_step], K).mean())
+    cg.close()
+    return {
+        "metric": "QPS at recall@10>=0.95 (plain bit-exact form)",
+        "value": round(qps, 1), "unit": "queries/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)",
+        "config": {"workload": WORKLOAD, "n": N_BASE, "dim": DIM, "k": K, "ef": ef_op,
+                   "step": f"{per_step} queries"},
+        "impl": "reference",
+        "recall_at_10": round(rec, 4),
+        "ef_curve": curve,
+        "cpu_baseline": {"value": round(qps, 1), "unit": "queries/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{per_step} queries per step, Graph::search (graph.h:33) from "
+                                   f"oracle/_ref on {threads} threads, ef={ef_op}"},
+        "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main(argv=None):
+    global N_BASE, NQ
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--ref-step-queries", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--n", type=int, default=N_BASE, help="base size (profiling cases)")
+    ap.add_argument("--nq", type=int, default=NQ, help="queries per GPU (profiling cases)")
+    ap.add_argument("--ef", type=int, default=0, help="fixed queue size: skip the sweep")
+    ap.add_argument("--bf-words", type=int, default=1024, help="Bloom words with --ef")
+    args = ap.parse_args(argv)
+    N_BASE, NQ = args.n, args.nq
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, ws, rank, local)
+        else:
+            out = run_ours(args, ws, rank, local)
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -142,6 +142,22 @@ song_status song_search_device(song_index* index, const void* d_queries, int nq,
                                int ef_search, int32_t* d_ids, song_query_trace* d_traces,
                                void* stream);
 
+/*
+ * Build an NSW graph on the current GPU: the reference's insertion algorithm
+ * (kernalGraph.h:140-149 / hashKernelGraph.h:196-207 -- beam search from
+ * node 0 with EF_CONSTRUCTION, SEARCH_DEGREE forward edges, reverse edges
+ * with farthest-eviction up to FIXED_DEGREE) run in batches of
+ * max(1, inserted/batch_ratio) nodes.  Same graph shape and rules, not
+ * byte-identical to the reference's sequential build.
+ * rows: FP32 [n x dim] (kind SONG_KIND_L2) or u32 codes [n x dim]
+ * (SONG_KIND_HAMMING), host.  adj_out: host [n x block_size].
+ * batch_ratio <= 0 selects 32; build_bf_words <= 0 selects 1024.
+ * fixed_degree must be <= 32 and <= block_size.
+ */
+song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
+                             const song_params* params, int batch_ratio, int build_bf_words,
+                             int32_t* adj_out);
+
 /* Number of search-kernel launches issued by this library since load. */
 int64_t song_kernel_launch_count(void);
 

@@ -78,6 +78,9 @@ DEFAULT_VARIANTS = [
     RefVariant(pq_size=512),
     RefVariant(pq_size=512, hash_bits=512),
     RefVariant(),
+    # the benchmark's operating points (queue cap 1024)
+    RefVariant(pq_size=1024, bf_words=256),
+    RefVariant(pq_size=1024, bf_words=1024),
 ]
 
 
