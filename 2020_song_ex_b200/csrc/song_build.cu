@@ -208,3 +208,123 @@ cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim,
 }
 
 }  // namespace song
+
+namespace song {
+
+namespace {
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+struct BuildScratch {
+    unsigned* ctr;
+    int* err;
+    int32_t* fwd;
+    uint32_t *k0, *k1, *v0, *v1;
+    void* tmp;
+    size_t tmp_bytes;
+    size_t total;
+};
+
+// Carves the build temporaries out of one region starting at `base` (or, for
+// base == nullptr, only computes the layout and the total size).
+cudaError_t carve_build_scratch(int64_t n, const song_params& p, int ratio, char* base,
+                                BuildScratch* s, int* key_bits) {
+    const int64_t maxB = std::max<int64_t>(1, (n - 1) / ratio + 1);
+    const int64_t maxE = maxB * p.search_degree;
+    if (maxE > (int64_t)INT32_MAX / 2) return cudaErrorInvalidValue;  // far beyond any scratch
+    int kb = 1;
+    while (kb < 32 && ((int64_t)1 << kb) <= n) ++kb;
+    *key_bits = kb;
+    size_t tmp_bytes = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint32_t*)nullptr,
+                                                    (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                                    (uint32_t*)nullptr, (int)maxE, 0, kb);
+    if (e != cudaSuccess) return e;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += align256(bytes); return base ? base + o : nullptr; };
+    s->ctr = reinterpret_cast<unsigned*>(take(8));
+    s->err = s->ctr ? reinterpret_cast<int*>(s->ctr + 1) : nullptr;
+    s->fwd = reinterpret_cast<int32_t*>(take((size_t)maxE * 4));
+    s->k0 = reinterpret_cast<uint32_t*>(take((size_t)maxE * 4));
+    s->k1 = reinterpret_cast<uint32_t*>(take((size_t)maxE * 4));
+    s->v0 = reinterpret_cast<uint32_t*>(take((size_t)maxE * 4));
+    s->v1 = reinterpret_cast<uint32_t*>(take((size_t)maxE * 4));
+    s->tmp = take(tmp_bytes);
+    s->tmp_bytes = tmp_bytes;
+    s->total = off;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+size_t build_scratch_bytes(int64_t n, const song_params& p, int ratio) {
+    if (ratio < 1) ratio = 32;
+    BuildScratch s{};
+    int kb = 0;
+    if (carve_build_scratch(n, p, ratio, nullptr, &s, &kb) != cudaSuccess) return (size_t)-1;
+    return s.total;
+}
+
+// The batched build of build_graph_device with every temporary taken from
+// the caller's device region `scratch` (build_scratch_bytes(n, p, ratio)
+// bytes) instead of cudaMalloc.  Stream-ordered on `st`; does not wait.
+cudaError_t build_graph_with_scratch(int kind, const void* d_base, int64_t n, int dim, int ld,
+                                     const song_params& p, int ratio, int bf_words,
+                                     int32_t* d_adj, int num_sms, cudaStream_t st, void* scratch,
+                                     size_t scratch_bytes) {
+    if (ratio < 1) ratio = 32;
+    const int bs = p.block_size, fd = p.fixed_degree, sd = p.search_degree;
+    if (fd > 32 || fd > bs || sd < 1) return cudaErrorInvalidValue;
+    BuildScratch s{};
+    int key_bits = 0;
+    cudaError_t e = carve_build_scratch(n, p, ratio, static_cast<char*>(scratch), &s, &key_bits);
+    if (e != cudaSuccess) return e;
+    if (s.total > scratch_bytes) return cudaErrorInvalidValue;
+    e = cudaMemsetAsync(d_adj, 0xff, (size_t)n * bs * sizeof(int32_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.ctr, 0, 8, st);  // counter and error word
+    int64_t u = 1;
+    while (e == cudaSuccess && u < n) {
+        const int B = (int)std::min<int64_t>(n - u, std::max<int64_t>(1, u / ratio));
+        SearchArgs a{};
+        a.base = d_base;
+        a.adj = d_adj;
+        a.queries = static_cast<const char*>(d_base) + (size_t)u * ld * 4;
+        a.out = s.fwd;
+        a.counter = s.ctr;
+        a.err = s.err;
+        a.n = u;
+        a.dim = dim;
+        a.ld = ld;
+        a.qld = ld;
+        a.block_size = bs;
+        a.k = sd;
+        a.nq = B;
+        a.cap = std::max(1, p.ef_construction);
+        a.bf_words = bf_words;
+        a.bf_nhash = 4;
+        a.n_multiprobe = 1;
+        search_warp_smem(kind, dim, a.cap, bf_words, &a);
+        e = cudaMemsetAsync(s.ctr, 0, 4, st);
+        if (e == cudaSuccess) e = launch_search(kind, a, num_sms, st);
+        if (e != cudaSuccess) break;
+        const int64_t cells = (int64_t)B * bs;
+        scatter_forward<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(s.fwd, sd, fd, bs, u, B,
+                                                                          d_adj, s.k0, s.v0);
+        const int E = B * sd;
+        size_t tb = s.tmp_bytes;
+        e = cub::DeviceRadixSort::SortPairs(s.tmp, tb, s.k0, s.k1, s.v0, s.v1, E, 0, key_bits, st);
+        if (e != cudaSuccess) break;
+        const int64_t threads = (int64_t)E * 32;
+        if (kind == SONG_KIND_L2)
+            reverse_edges<SONG_KIND_L2><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+                s.k1, s.v1, E, d_base, ld, dim, d_adj, bs, fd);
+        else
+            reverse_edges<SONG_KIND_HAMMING><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+                s.k1, s.v1, E, d_base, ld, dim, d_adj, bs, fd);
+        e = cudaGetLastError();
+        u += B;
+    }
+    return e;
+}
+
+}  // namespace song

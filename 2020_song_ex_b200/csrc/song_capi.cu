@@ -315,6 +315,10 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
 
 }  // namespace
 
+namespace song {
+song_status set_error(song_status status, const char* message) { return fail(status, message); }
+}  // namespace song
+
 extern "C" {
 
 void song_params_default(song_params* p) {

@@ -43,4 +43,17 @@ cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim,
                                const song_params& p, int ratio, int bf_words, int32_t* d_adj,
                                int num_sms, cudaStream_t st);
 
+// Scratch bytes build_graph_with_scratch needs for (n, params, ratio).
+size_t build_scratch_bytes(int64_t n, const song_params& p, int ratio);
+
+// build_graph_device with all temporaries carved from caller scratch; no
+// allocation, stream-ordered, does not wait.
+cudaError_t build_graph_with_scratch(int kind, const void* d_base, int64_t n, int dim, int ld,
+                                     const song_params& p, int ratio, int bf_words,
+                                     int32_t* d_adj, int num_sms, cudaStream_t st, void* scratch,
+                                     size_t scratch_bytes);
+
+// Records a failure message for song_last_error() on the calling thread.
+song_status set_error(song_status status, const char* message);
+
 }  // namespace song

@@ -158,6 +158,26 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
                              const song_params* params, int batch_ratio, int build_bf_words,
                              int32_t* adj_out);
 
+/*
+ * Allocation-free song_build_graph (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc while they build a graph: a
+ * serving process whose device memory is owned by its own pool, or one that
+ * must not let an allocation synchronise the device under live traffic.
+ * d_rows ([n x ld] FP32 or u32 codes, ld a multiple of 4, 16-byte aligned)
+ * and d_adj ([n x block_size], written) are the caller's device buffers; all
+ * temporaries live in one fixed 16 MiB device array inside this library,
+ * which every GPU that loads the library holds until the process exits.  A
+ * build whose temporaries do not fit is rejected with SONG_ERR_BUDGET (the
+ * message gives the bytes needed; a larger batch_ratio needs less).
+ * Asynchronous on `stream` (a cudaStream_t).  The first call on a device
+ * looks up the array's device address, so make that first call before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race with each other.  Produces the same graph as song_build_graph.
+ */
+song_status song_build_graph_noalloc(int kind, const void* d_rows, int64_t n, int dim, int ld,
+                                     const song_params* params, int batch_ratio,
+                                     int build_bf_words, int32_t* d_adj, void* stream);
+
 /* Number of search-kernel launches issued by this library since load. */
 int64_t song_kernel_launch_count(void);
 
