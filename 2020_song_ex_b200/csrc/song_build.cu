@@ -127,7 +127,7 @@ __global__ void reverse_edges(const uint32_t* __restrict__ keys, const uint32_t*
 // ([n x ld], kind L2 or Hamming).  Stream-ordered; returns a CUDA error.
 cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim, int ld,
                                const song_params& p, int ratio, int bf_words, int32_t* d_adj,
-                               int num_sms, cudaStream_t st) {
+                               int num_sms, cudaStream_t st, BaseRange range) {
     if (ratio < 1) ratio = 32;
     const int bs = p.block_size, fd = p.fixed_degree, sd = p.search_degree;
     if (fd > 32 || fd > bs || sd < 1) return cudaErrorInvalidValue;
@@ -182,6 +182,9 @@ cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim,
         a.bf_words = bf_words;
         a.bf_nhash = 4;
         a.n_multiprobe = 1;  // the reference build search starts from node 0 alone
+        a.int_base = range.int_base;
+        a.base_min = range.lo;
+        a.base_max = range.hi;
         search_warp_smem(kind, dim, a.cap, bf_words, &a);
         e = cudaMemsetAsync(ctr, 0, 4, st);
         if (e == cudaSuccess) e = launch_search(kind, a, num_sms, st);

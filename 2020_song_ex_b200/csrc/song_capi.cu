@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -34,6 +35,7 @@ struct song_index {
     int64_t n = 0;
     int dim = 0;  // floats (L2) or u32 words (Hamming) per vector
     int ld = 0;   // padded row stride in elements (multiple of 4)
+    song::BaseRange range;  // integer range of the base (L2), for the exact-integer path
     song_params p{};
     int device = 0;
     int num_sms = 0;
@@ -145,8 +147,9 @@ song_status create_common(int kind, const void* rows, int64_t n, int dim, const 
     x->kind = kind;
     x->n = n;
     x->dim = dim;
-    x->ld = round_up4(dim);
+    x->ld = song::search_row_stride(kind, dim);
     x->p = *params;
+    if (kind == SONG_KIND_L2) x->range = song::scan_base_range((const float*)rows, n, dim);
     cudaError_t e = cudaGetDevice(&x->device);
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, x->device);
@@ -215,7 +218,12 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
     a->bf_words = x->p.bf_words;
     a->bf_nhash = x->p.bf_nhash;
     a->n_multiprobe = x->p.n_multiprobe;
+    a->int_base = x->range.int_base;
+    a->base_min = x->range.lo;
+    a->base_max = x->range.hi;
     song::search_warp_smem(x->kind, x->dim, cap, x->p.bf_words, a);
+    if (cap > 4096)
+        return fail(SONG_ERR_UNSUPPORTED, "queue capacity above 4096 slots (pq_size and ef) is not supported");
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, x->device);
     if (a->warp_smem > optin) {
@@ -317,6 +325,27 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
 
 namespace song {
 song_status set_error(song_status status, const char* message) { return fail(status, message); }
+
+BaseRange scan_base_range(const float* rows, int64_t n, int dim) {
+    BaseRange r;
+    const int64_t total = n * (int64_t)dim;
+    if (total <= 0) return r;
+    float lo = rows[0], hi = rows[0];
+    bool integral = true;
+    for (int64_t i = 0; i < total; ++i) {
+        const float v = rows[i];
+        if (!(v == std::nearbyint(v)) || !(std::fabs(v) < 16777216.0f)) {
+            integral = false;
+            break;
+        }
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+    }
+    r.int_base = integral ? 1 : 0;
+    r.lo = lo;
+    r.hi = hi;
+    return r;
+}
 }  // namespace song
 
 extern "C" {
@@ -406,7 +435,9 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
         params->ef_construction < 1)
         return fail(SONG_ERR_UNSUPPORTED, "GPU build needs 1 <= fixed_degree <= min(32, block_size)");
     const int bfw = build_bf_words > 0 ? build_bf_words : 1024;
-    const int ld = round_up4(dim);
+    const int ld = song::search_row_stride(kind, dim);
+    const song::BaseRange range =
+        kind == SONG_KIND_L2 ? song::scan_base_range((const float*)rows, n, dim) : song::BaseRange();
     int dev = 0, sms = 0;
     SONG_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
     SONG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
@@ -423,7 +454,7 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
                          cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = song::build_graph_device(kind, d_rows, n, dim, ld, *params, batch_ratio, bfw, d_adj,
-                                     sms, st);
+                                     sms, st, range);
     if (e == cudaSuccess)
         e = cudaMemcpy(adj_out, d_adj, (size_t)n * params->block_size * 4, cudaMemcpyDeviceToHost);
     cudaFree(d_rows);

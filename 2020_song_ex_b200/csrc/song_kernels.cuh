@@ -28,8 +28,20 @@ struct SearchArgs {
     int bf_nhash;            // BF_NHASH (1..4)
     int n_multiprobe;        // N_MULTIPROBE
     int warp_smem;           // bytes of shared memory per warp (multiple of 16)
-    int q_off, cd_off, ci_off, rd_off, ri_off, bl_off;  // per-warp carve-up, bytes
+    int q_off, rows_off, cd_off, ci_off, rd_off, ri_off, bl_off;  // per-warp carve-up, bytes
+    int int_base;            // 1: every base value is an integer in [base_min, base_max]
+    float base_min, base_max;
 };
+
+// Integer range of FP32 rows (0 in int_base if any value is not an integer).
+struct BaseRange {
+    int int_base = 0;
+    float lo = 0.0f, hi = 0.0f;
+};
+BaseRange scan_base_range(const float* rows, int64_t n, int dim);
+
+// Row stride (elements) the kernels use for `dim` elements of `kind`.
+int search_row_stride(int kind, int dim);
 
 // Per-warp shared-memory layout for (kind, dim, cap, bf_words).
 int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a);
@@ -41,7 +53,7 @@ cudaError_t launch_search(int kind, const SearchArgs& a, int num_sms, cudaStream
 // Batched-insertion NSW build over device rows (song_build.cu).
 cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim, int ld,
                                const song_params& p, int ratio, int bf_words, int32_t* d_adj,
-                               int num_sms, cudaStream_t st);
+                               int num_sms, cudaStream_t st, BaseRange range = BaseRange());
 
 // Scratch bytes build_graph_with_scratch needs for (n, params, ratio).
 size_t build_scratch_bytes(int64_t n, const song_params& p, int ratio);

@@ -79,6 +79,9 @@ song_status song_build_graph_noalloc(int kind, const void* d_rows, int64_t n, in
     if (dim < 1 || ld < dim || ld % 4 != 0 || (kind == SONG_KIND_HAMMING && dim > 32))
         return song::set_error(SONG_ERR_INVALID_ARG,
                                "need 1 <= dim <= ld, ld a multiple of 4 (and dim <= 32 for codes)");
+    if (kind == SONG_KIND_HAMMING && ld != song::search_row_stride(kind, dim))
+        return song::set_error(SONG_ERR_INVALID_ARG,
+                               "for codes, ld must be 4, 8, 16 or 32 words (the smallest >= dim)");
     if (((uintptr_t)d_rows & 15u) != 0)
         return song::set_error(SONG_ERR_INVALID_ARG, "d_rows must be 16-byte aligned");
     if (params->block_size < 1 || params->fixed_degree < 1 || params->fixed_degree > 32 ||

@@ -1,30 +1,39 @@
 // song_search.cu -- sm_100a kernels of the plain SONG graph search.
 //
-// One warp owns one query at a time; W warps share a CTA and a persistent
-// grid pulls queries from a device work counter, so every SM keeps many
-// independent traversals (and their neighbour gathers) in flight.  The
-// reference runs one query per single-warp block with lane 0 doing all queue
-// and Bloom work serially (kernalGraph.h:184-299).
+// One warp owns one query at a time; several warps share a CTA and a
+// persistent grid pulls queries from a device work counter, so every SM
+// keeps many independent traversals (and their neighbour gathers) in flight.
+// The reference runs one query per single-warp block with lane 0 doing all
+// queue and Bloom work serially (kernalGraph.h:184-299).
 //
 // Results are bit-exact with the reference, including tie order and the
 // QueryTrace counters, because the per-query state is the reference's own
 // state and every step keeps its order:
 //  * Candidates / Results (gpuHeap.h:8-108) stay unsorted slot arrays in
-//    shared memory with the same slot moves.  Their O(cap) scans become
-//    warp scans + redux.sync argmin/argmax that break ties by the lowest
-//    slot, i.e. the reference's "first index" rule (strict < / strict >).
+//    shared memory with exactly the reference's slot moves.  The O(cap)
+//    scans become a two-level tournament: slots are grouped 32 at a time
+//    (one slot per lane), each group's (max, first slot) and (min, first
+//    slot) summary lives in a register of lane g, and "first maximal slot"
+//    or "first minimal slot" is two redux.sync over those summaries.  A slot
+//    write refreshes only its group (one shared load per lane + redux).
+//    Ties break on the lowest slot -- the reference's first-index rule.
 //  * A row of up to 32 neighbours is handled at once, lane j = slot j, but
-//    the Bloom test of neighbour j sees the bits of neighbours < j exactly
-//    as bf_test/bf_set in j order do (bloomFilter.h:34-48): see bloom_chunk.
+//    the Bloom test of neighbour j sees the bits of neighbours < j exactly as
+//    bf_test/bf_set in j order do (bloomFilter.h:34-48): see bloom_chunk.
 //  * Distances follow warp_l2 (kernalGraph.h:157-170): lane l sums
 //    (q_i - b_i)^2 over i = l (mod 32) with FMA, then a butterfly
-//    transpose-reduce over 32 rows whose association is exactly the
-//    reference's shfl_down tree (16,8,4,2,1), so FP32 sums match for any
-//    data; lane j ends holding the distance of row j.
+//    transpose-reduce whose association is the reference's shfl_down tree.
+//    When every term and partial sum is an integer below 2^24 (integer
+//    vectors, the SIFT-shaped case) every order gives the same FP32 value,
+//    so those queries take a gather-only path instead: 8 lanes per row,
+//    16-byte loads, only the rows that passed the Bloom test.
 //  * Pushes are applied in lane (= j) order; a push into a full queue only
 //    evicts when strictly closer than the current first maximum, and the
 //    maximum never grows while a queue is full, so lanes that lose against
 //    the running maximum drop out with one ballot.
+//  * The final trim (pop_worst) and drain (drain_best) are replayed exactly;
+//    when the k+1 smallest results have distinct distances their outcome is
+//    simply those k in ascending order, which is taken directly.
 #include <algorithm>
 #include <atomic>
 #include <climits>
@@ -38,6 +47,7 @@ std::atomic<int64_t> g_launches{0};
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
+constexpr unsigned NONE = 0xffffffffu;  // "no slot" / empty group
 
 // The mixing constants of bloomFilter.h:14-19: two per hash function.
 __constant__ uint64_t kBloomMix[8] = {
@@ -45,93 +55,164 @@ __constant__ uint64_t kBloomMix[8] = {
     0x3a7b976128a30449ULL, 0x6d122efabfc4d99fULL, 0xe6700ef8715030e2ULL, 0x80dd0c3bffcfb45bULL,
 };
 
-// A bounded slot queue in shared memory; the scalar fields are warp-uniform.
+__device__ __forceinline__ unsigned fbits(float x) { return __float_as_uint(x); }
+__device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+// Slot queue of capacity <= 1024 * GPL.  Slots live in shared memory; the
+// summary of group g (slots 32g .. 32g+31) is held by lane g % 32 in entry
+// g / 32.  Distances are non-negative, so their bit patterns order like the
+// floats.  All scalar fields are warp-uniform.
+template <int GPL>
 struct Queue {
     float* d;
     int* id;
     int sz;
     int cap;
-    float maxv;   // first maximal slot (valid when max_ok)
-    int maxi;
-    bool max_ok;
+    unsigned xb[GPL], xi[GPL];  // group maximum bits, first slot holding it (NONE = empty)
+    unsigned nb[GPL], ni[GPL];  // group minimum bits, first slot holding it
 };
 
-struct BloomCfg {
-    uint64_t nbits;     // BF_WORDS * 64
-    uint32_t words;     // BF_WORDS
-    uint32_t wmask;     // BF_WORDS - 1 when a power of two
-    int shift;          // log2(BF_WORDS), or -1
-    int nhash;          // BF_NHASH
-};
-
-__device__ __forceinline__ unsigned fbits(float x) { return __float_as_uint(x); }
-
-// First slot holding the minimum over [0, sz).  Distances are non-negative,
-// so their bit patterns order like the floats.
-__device__ __forceinline__ void q_argmin(const Queue& q, int lane, float& v, int& idx) {
-    unsigned best = 0xffffffffu, bi = 0xffffffffu;
-    for (int s = lane; s < q.sz; s += 32) {
-        const unsigned b = fbits(q.d[s]);
-        if (b < best) { best = b; bi = (unsigned)s; }
+template <int GPL>
+__device__ __forceinline__ void q_init(Queue<GPL>& q, float* d, int* id, int cap) {
+    q.d = d;
+    q.id = id;
+    q.sz = 0;
+    q.cap = cap;
+#pragma unroll
+    for (int r = 0; r < GPL; ++r) {
+        q.xb[r] = 0u;
+        q.xi[r] = NONE;
+        q.nb[r] = 0xffffffffu;
+        q.ni[r] = NONE;
     }
-    const unsigned m = __reduce_min_sync(FULL, best);
-    idx = (int)__reduce_min_sync(FULL, best == m ? bi : 0xffffffffu);
-    v = __uint_as_float(m);
+}
+
+// Refresh the summary of group g from the slot array.  MIN: also the minimum.
+template <bool MIN, int GPL>
+__device__ __forceinline__ void group_update(Queue<GPL>& q, int g, int lane) {
+    const int s = (g << 5) + lane;
+    const bool occ = s < q.sz;
+    const unsigned b = occ ? fbits(q.d[s]) : 0u;
+    const unsigned mx = __reduce_max_sync(FULL, b);
+    const unsigned mxi = __reduce_min_sync(FULL, (occ && b == mx) ? (unsigned)s : NONE);
+    unsigned mn = 0xffffffffu, mni = NONE;
+    if constexpr (MIN) {
+        mn = __reduce_min_sync(FULL, occ ? b : 0xffffffffu);
+        mni = __reduce_min_sync(FULL, (occ && b == mn) ? (unsigned)s : NONE);
+    }
+    if ((g & 31) == lane) {
+        const int r = g >> 5;
+#pragma unroll
+        for (int t = 0; t < GPL; ++t) {
+            if (t == r) {
+                q.xb[t] = mx;
+                q.xi[t] = mxi;
+                if constexpr (MIN) {
+                    q.nb[t] = mn;
+                    q.ni[t] = mni;
+                }
+            }
+        }
+    }
 }
 
 // First slot holding the maximum over [0, sz) (gpuHeap.h:29, :73, :83, :93).
-__device__ __forceinline__ void q_argmax(Queue& q, int lane) {
-    unsigned best = 0u, bi = 0xffffffffu;
-    for (int s = lane; s < q.sz; s += 32) {
-        const unsigned b = fbits(q.d[s]);
-        if (bi == 0xffffffffu || b > best) { best = b; bi = (unsigned)s; }
+template <int GPL>
+__device__ __forceinline__ void root_max(const Queue<GPL>& q, unsigned& mb, unsigned& mi) {
+    unsigned b = 0u, i = NONE;
+#pragma unroll
+    for (int r = 0; r < GPL; ++r)
+        if (q.xi[r] != NONE && (i == NONE || q.xb[r] > b)) {
+            b = q.xb[r];
+            i = q.xi[r];
+        }
+    mb = __reduce_max_sync(FULL, i != NONE ? b : 0u);
+    mi = __reduce_min_sync(FULL, (i != NONE && b == mb) ? i : NONE);
+}
+
+// First slot holding the minimum over [0, sz) (gpuHeap.h:42, :263).
+template <int GPL>
+__device__ __forceinline__ void root_min(const Queue<GPL>& q, unsigned& mb, unsigned& mi) {
+    unsigned b = 0xffffffffu, i = NONE;
+#pragma unroll
+    for (int r = 0; r < GPL; ++r)
+        if (q.ni[r] != NONE && (i == NONE || q.nb[r] < b)) {
+            b = q.nb[r];
+            i = q.ni[r];
+        }
+    mb = __reduce_min_sync(FULL, i != NONE ? b : 0xffffffffu);
+    mi = __reduce_min_sync(FULL, (i != NONE && b == mb) ? i : NONE);
+}
+
+// Move the last slot into slot `hole` and shrink (the removal of
+// Candidates::pop_min, Results::pop_worst and drain_best).
+template <bool MIN, int GPL>
+__device__ __forceinline__ void q_remove(Queue<GPL>& q, int hole, int lane) {
+    const int last = q.sz - 1;
+    __syncwarp();
+    if (lane == 0 && hole != last) {
+        q.d[hole] = q.d[last];
+        q.id[hole] = q.id[last];
     }
-    const unsigned m = __reduce_max_sync(FULL, best);
-    q.maxi = (int)__reduce_min_sync(FULL, (bi != 0xffffffffu && best == m) ? bi : 0xffffffffu);
-    q.maxv = __uint_as_float(m);
-    q.max_ok = true;
+    __syncwarp();
+    q.sz = last;
+    group_update<MIN>(q, hole >> 5, lane);
+    if ((last >> 5) != (hole >> 5)) group_update<MIN>(q, last >> 5, lane);
 }
 
 // Push (d, nb) of every lane in N, in lane order, with the semantics of
 // Candidates::push / Results::try_push (gpuHeap.h:23-36, :68-77).
 // Returns how many pushes were accepted.
-__device__ __forceinline__ int q_push(Queue& q, unsigned N, float d, int nb, int lane) {
+template <bool MIN, int GPL>
+__device__ __forceinline__ int q_push(Queue<GPL>& q, unsigned N, float d, int nb, int lane) {
     if (N == 0u) return 0;
     const bool mine = (N >> lane) & 1u;
-    const int rank = __popc(N & ((1u << lane) - 1u));
+    const int rank = __popc(N & lanemask_lt(lane));
     const int nm = __popc(N);
     const int room = q.cap - q.sz;
-    if (mine && rank < room) {
-        q.d[q.sz + rank] = d;
-        q.id[q.sz + rank] = nb;
-    }
-    int accepted = nm < room ? nm : room;
-    if (accepted > 0) {
-        q.sz += accepted;
-        q.max_ok = false;
+    int acc = 0;
+    if (room > 0) {
+        const int a = nm < room ? nm : room;
+        if (mine && rank < a) {
+            q.d[q.sz + rank] = d;
+            q.id[q.sz + rank] = nb;
+        }
+        __syncwarp();
+        const int g0 = q.sz >> 5, g1 = (q.sz + a - 1) >> 5;
+        q.sz += a;
+        for (int g = g0; g <= g1; ++g) group_update<MIN>(q, g, lane);
+        acc = a;
     }
     if (nm > room) {
-        __syncwarp();
-        if (!q.max_ok) q_argmax(q, lane);
-        unsigned rest = __ballot_sync(FULL, mine && rank >= room && d < q.maxv);
+        unsigned M, fi;
+        root_max(q, M, fi);
+        unsigned rest = __ballot_sync(FULL, mine && rank >= room && fbits(d) < M);
         while (rest) {
             const int j = __ffs(rest) - 1;
             const float dj = __shfl_sync(FULL, d, j);
             const int nj = __shfl_sync(FULL, nb, j);
             if (lane == 0) {
-                q.d[q.maxi] = dj;
-                q.id[q.maxi] = nj;
+                q.d[fi] = dj;
+                q.id[fi] = nj;
             }
             __syncwarp();
-            ++accepted;
-            q_argmax(q, lane);
+            group_update<MIN>(q, (int)(fi >> 5), lane);
+            ++acc;
+            root_max(q, M, fi);
             rest &= ~(1u << j);
-            rest &= __ballot_sync(FULL, d < q.maxv);
+            rest &= __ballot_sync(FULL, fbits(d) < M);
         }
     }
-    __syncwarp();
-    return accepted;
+    return acc;
 }
+
+struct BloomCfg {
+    uint64_t nbits;  // BF_WORDS * 64
+    uint32_t words;  // BF_WORDS
+    uint32_t wmask;  // BF_WORDS - 1 when a power of two
+    int shift;       // log2(BF_WORDS), or -1
+    int nhash;       // BF_NHASH
+};
 
 // bf_hash (bloomFilter.h:23-30) for a node id x >= 0.  The first x ^= x>>33
 // of the reference is the identity for x < 2^33 and is left out.
@@ -244,12 +325,12 @@ __device__ __forceinline__ float row_partial(const float* __restrict__ row, int 
     return s;
 }
 
-// Squared L2 distances of the rows of the lanes in N; lane j returns the
-// distance of its own row (meaningful when bit j of N is set).  Partial sums
-// are combined by a butterfly transpose-reduce: step w (16,8,4,2,1) pairs
-// lanes l and l^w, which is the reference tree's pairing of m and m+w.
+// Squared L2 in the reference's exact order for the rows of the lanes in N;
+// lane j returns the distance of its own row.  Partial sums are combined by
+// a butterfly transpose-reduce: step w (16,8,4,2,1) pairs lanes l and l^w,
+// which is the reference tree's pairing of m and m+w.
 template <int NE>
-__device__ __forceinline__ float l2_chunk(const float* __restrict__ base, int ld, int dim,
+__device__ __forceinline__ float l2_exact(const float* __restrict__ base, int ld, int dim,
                                           const float (&qreg)[NE > 0 ? NE : 1], const float* sq,
                                           int nb, unsigned N, int lane) {
     float v[16];
@@ -278,6 +359,59 @@ __device__ __forceinline__ float l2_chunk(const float* __restrict__ base, int ld
     return v[0];
 }
 
+// Squared L2 when every partial sum is an exact integer (any order gives the
+// same FP32 value): only the rows of the lanes in N are gathered, 4 rows per
+// pass with 8 lanes per row and NV 16-byte loads per lane (dim = 32 * NV),
+// two passes in flight.  `rows` is a 32-entry per-warp shared list.
+template <int NV>
+__device__ __forceinline__ float l2_int(const float* __restrict__ base, int ld,
+                                        const float4 (&qv)[NV], int nb, unsigned N,
+                                        int* rows, int lane) {
+    const bool mine = (N >> lane) & 1u;
+    const int rank = __popc(N & lanemask_lt(lane));
+    const int m = __popc(N);
+    if (mine) rows[rank] = nb;
+    __syncwarp();
+    const int grp = lane >> 3, t = lane & 7;
+    float out = 0.0f;
+    for (int p0 = 0; p0 < m; p0 += 8) {
+        const int ra = p0 + grp, rb = p0 + 4 + grp;
+        float4 xa[NV], xb[NV];
+        const bool va = ra < m, vb = rb < m;
+        const float4* pa = reinterpret_cast<const float4*>(base + (size_t)(va ? rows[ra] : 0) * ld);
+        const float4* pb = reinterpret_cast<const float4*>(base + (size_t)(vb ? rows[rb] : 0) * ld);
+#pragma unroll
+        for (int e = 0; e < NV; ++e) xa[e] = va ? __ldg(pa + t + 8 * e) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int e = 0; e < NV; ++e) xb[e] = vb ? __ldg(pb + t + 8 * e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        float sa = 0.0f, sb = 0.0f;
+#pragma unroll
+        for (int e = 0; e < NV; ++e) {
+            float u;
+            u = qv[e].x - xa[e].x; sa = fmaf(u, u, sa);
+            u = qv[e].y - xa[e].y; sa = fmaf(u, u, sa);
+            u = qv[e].z - xa[e].z; sa = fmaf(u, u, sa);
+            u = qv[e].w - xa[e].w; sa = fmaf(u, u, sa);
+            u = qv[e].x - xb[e].x; sb = fmaf(u, u, sb);
+            u = qv[e].y - xb[e].y; sb = fmaf(u, u, sb);
+            u = qv[e].z - xb[e].z; sb = fmaf(u, u, sb);
+            u = qv[e].w - xb[e].w; sb = fmaf(u, u, sb);
+        }
+#pragma unroll
+        for (int w = 4; w >= 1; w >>= 1) {
+            sa += __shfl_xor_sync(FULL, sa, w);
+            sb += __shfl_xor_sync(FULL, sb, w);
+        }
+        // row of rank r sits in group r % 4 of pass r / 4
+        const float ga = __shfl_sync(FULL, sa, (rank & 3) << 3);
+        const float gb = __shfl_sync(FULL, sb, (rank & 3) << 3);
+        if (mine && (rank >> 2) == (p0 >> 2)) out = ga;
+        if (mine && (rank >> 2) == (p0 >> 2) + 1) out = gb;
+    }
+    __syncwarp();
+    return out;
+}
+
 // Hamming distance of this lane's own row: popcount(q ^ b) over W4 uint4
 // (warp_hamming, hashKernelGraph.h:215-224; integer, so order-free).
 template <int W4>
@@ -296,17 +430,68 @@ __device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int
     return (float)s;
 }
 
-// KIND 0 = L2 with NE query elements per lane in registers (0: shared
-// memory); KIND 1 = Hamming with NE uint4 of code per row.
-template <int KIND, int NE>
+// Writes the k results (kernalGraph.h:292-296): `while (sz > k) pop_worst()`
+// then `drain_best(out, k)`, -1 padding.  The k+1 smallest results are
+// extracted first (into the free candidate arrays); if their distances are
+// strictly increasing the replay's outcome is exactly those k in order.
+// Otherwise the extraction is undone and the trims and drains are replayed.
+template <int GPL>
+__device__ __forceinline__ int finish(Queue<GPL>& res, Queue<GPL>& cand, int k, int32_t* out,
+                                      int lane) {
+    const int ng = (res.sz + 31) >> 5;
+    for (int g = 0; g < ng; ++g) group_update<true>(res, g, lane);
+    const int cnt = res.sz < k ? res.sz : k;
+    const int take = res.sz < k + 1 ? res.sz : k + 1;
+    unsigned* xv = reinterpret_cast<unsigned*>(cand.d);  // extracted distance bits
+    int* xs = cand.id;                                   // their slots
+    for (int i = 0; i < take; ++i) {
+        unsigned mb, mi;
+        root_min(res, mb, mi);
+        if (lane == 0) {
+            xv[i] = mb;
+            xs[i] = (int)mi;
+            reinterpret_cast<unsigned*>(res.d)[mi] = 0xffffffffu;  // out of every minimum
+        }
+        __syncwarp();
+        group_update<true>(res, (int)(mi >> 5), lane);
+    }
+    bool distinct = true;
+    for (int i = lane; i + 1 < take; i += 32) distinct &= xv[i] < xv[i + 1];
+    distinct = __all_sync(FULL, distinct);
+    if (distinct) {
+        for (int i = lane; i < cnt; i += 32) out[i] = res.id[xs[i]];
+    } else {
+        for (int i = lane; i < take; i += 32) reinterpret_cast<unsigned*>(res.d)[xs[i]] = xv[i];
+        __syncwarp();
+        for (int g = 0; g < ng; ++g) group_update<true>(res, g, lane);
+        while (res.sz > k) {  // Results::pop_worst
+            unsigned mb, mi;
+            root_max(res, mb, mi);
+            q_remove<true>(res, (int)mi, lane);
+        }
+        for (int i = 0; i < cnt; ++i) {  // Results::drain_best
+            unsigned mb, mi;
+            root_min(res, mb, mi);
+            const int id = res.id[mi];
+            if (lane == 0) out[i] = id;
+            q_remove<true>(res, (int)mi, lane);
+        }
+    }
+    for (int i = cnt + lane; i < k; i += 32) out[i] = -1;
+    return cnt;
+}
+
+// KIND 0 = L2 with NE query elements per lane (0: query in shared memory);
+// KIND 1 = Hamming with NE uint4 of code per row.  GPL: queue groups per lane.
+template <int KIND, int NE, int GPL>
 __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsigned char* ws,
                                              int lane) {
-    Queue cand{reinterpret_cast<float*>(ws + a.cd_off), reinterpret_cast<int*>(ws + a.ci_off), 0,
-               a.cap, 0.0f, 0, false};
-    Queue res{reinterpret_cast<float*>(ws + a.rd_off), reinterpret_cast<int*>(ws + a.ri_off), 0,
-              a.cap, 0.0f, 0, false};
+    Queue<GPL> cand, res;
+    q_init(cand, reinterpret_cast<float*>(ws + a.cd_off), reinterpret_cast<int*>(ws + a.ci_off), a.cap);
+    q_init(res, reinterpret_cast<float*>(ws + a.rd_off), reinterpret_cast<int*>(ws + a.ri_off), a.cap);
     uint64_t* bloom = reinterpret_cast<uint64_t*>(ws + a.bl_off);
     float* sq = reinterpret_cast<float*>(ws + a.q_off);
+    int* rows = reinterpret_cast<int*>(ws + a.rows_off);
 
     BloomCfg bc;
     bc.words = (uint32_t)a.bf_words;
@@ -315,16 +500,47 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     bc.wmask = (uint32_t)a.bf_words - 1u;
     bc.nhash = a.bf_nhash;
 
-    // Query: registers (and shared memory for the generic L2 path).
+    // Query in registers (and shared memory for the generic L2 path).
+    constexpr bool kIntPath = KIND == 0 && NE > 0;
     float qreg[(KIND == 0 && NE > 0) ? NE : 1];
+    float4 qv[kIntPath ? NE : 1];
     uint4 qcode[KIND == 1 ? NE : 1];
+    bool int_exact = false;
     if constexpr (KIND == 0) {
         const float* qg = reinterpret_cast<const float*>(a.queries) + (int64_t)qid * a.qld;
         if constexpr (NE > 0) {
+            float lo = INFINITY, hi = -INFINITY;
+            bool integral = true;
 #pragma unroll
             for (int e = 0; e < NE; ++e) {
                 const int i = lane + 32 * e;
                 qreg[e] = i < a.dim ? qg[i] : 0.0f;
+                if (i < a.dim) {
+                    lo = fminf(lo, qreg[e]);
+                    hi = fmaxf(hi, qreg[e]);
+                    integral &= qreg[e] == rintf(qreg[e]);
+                }
+            }
+            if (a.int_base && a.dim == 32 * NE) {
+                // every |q_i - b_i| <= maxd; dim * maxd^2 < 2^24 keeps all sums exact
+                integral = __all_sync(FULL, integral);
+#pragma unroll
+                for (int w = 16; w >= 1; w >>= 1) {
+                    lo = fminf(lo, __shfl_xor_sync(FULL, lo, w));
+                    hi = fmaxf(hi, __shfl_xor_sync(FULL, hi, w));
+                }
+                const double maxd = fmax((double)a.base_max - lo, (double)hi - a.base_min);
+                int_exact = integral && (double)a.dim * maxd * maxd < 16777216.0;
+                if (int_exact) {
+                    const float4* q4 = reinterpret_cast<const float4*>(qg);
+                    const bool aligned = ((reinterpret_cast<uintptr_t>(qg) & 15u) == 0);
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) {
+                        const int f = (lane & 7) + 8 * e;
+                        qv[e] = aligned ? q4[f]
+                                        : make_float4(qg[4 * f], qg[4 * f + 1], qg[4 * f + 2], qg[4 * f + 3]);
+                    }
+                }
             }
         } else {
             qreg[0] = 0.0f;
@@ -343,118 +559,82 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     for (int w = lane; w < a.bf_words; w += 32) bloom[w] = 0ull;
     __syncwarp();
 
-    auto dist = [&](int nb, unsigned N) -> float {
-        if constexpr (KIND == 0) {
-            return l2_chunk<NE>(reinterpret_cast<const float*>(a.base), a.ld, a.dim, qreg, sq, nb, N,
-                                lane);
-        } else {
-            return ham_lane<NE>(reinterpret_cast<const uint32_t*>(a.base), a.ld, qcode, nb,
-                                (N >> lane) & 1u);
-        }
-    };
-
     song_query_trace tr = {};
-
-    // Seeds p*n/N_MULTIPROBE, 64-bit product (kernalGraph.h:214-231).
-    for (int p0 = 0; p0 < a.n_multiprobe; p0 += 32) {
-        const int p = p0 + lane;
-        int ep = -1;
-        if (p < a.n_multiprobe)
-            ep = (int)((unsigned long long)p * (unsigned long long)a.n /
-                       (unsigned long long)a.n_multiprobe);
-        const unsigned N = bloom_chunk(bloom, ep, bc, lane);
-        const float d = dist(ep, N);
-        const int c = __popc(N);
-        tr.seed_count += c;
-        tr.visited_nodes += c;
-        tr.distance_evals += c;
-        tr.frontier_pushes += q_push(cand, N, d, ep, lane);
-        tr.result_updates += q_push(res, N, d, ep, lane);
-        if (N) {
-            tr.peak_frontier = max(tr.peak_frontier, cand.sz);
-            tr.peak_results = max(tr.peak_results, res.sz);
-        }
-    }
-
-    // Expansion loop (kernalGraph.h:233-289).
+    bool seeding = true;  // the first pass inserts the N_MULTIPROBE entry points
     for (;;) {
-        if (cand.sz == 0) break;
-        float cmin;
-        int mi;
-        q_argmin(cand, lane, cmin, mi);
-        const int cn = cand.id[mi];
-        __syncwarp();
-        if (lane == 0) {
-            cand.d[mi] = cand.d[cand.sz - 1];
-            cand.id[mi] = cand.id[cand.sz - 1];
-        }
-        cand.sz -= 1;
-        cand.max_ok = false;
-        __syncwarp();
-        tr.expanded_nodes += 1;
-        if (res.sz == res.cap) {  // early stop: full and strictly worse than the worst
-            if (!res.max_ok) q_argmax(res, lane);
-            if (cmin > res.maxv) {
-                tr.early_stopped = 1;
-                break;
+        int limit;
+        const int32_t* arow = nullptr;
+        if (seeding) {
+            limit = a.n_multiprobe;  // seeds p*n/N_MULTIPROBE (kernalGraph.h:214-231)
+        } else {                     // expansion (kernalGraph.h:233-289)
+            if (cand.sz == 0) break;
+            unsigned mb, mi;
+            root_min(cand, mb, mi);
+            const float cmin = __uint_as_float(mb);
+            const int cn = cand.id[mi];
+            q_remove<true>(cand, (int)mi, lane);
+            tr.expanded_nodes += 1;
+            if (res.sz == res.cap) {  // early stop: full and strictly worse than the worst
+                unsigned wb, wi;
+                root_max(res, wb, wi);
+                if (fbits(cmin) > wb) {
+                    tr.early_stopped = 1;
+                    break;
+                }
             }
+            limit = a.block_size;
+            arow = a.adj + (int64_t)cn * a.block_size;
         }
-        const int32_t* arow = a.adj + (int64_t)cn * a.block_size;
-        for (int c0 = 0; c0 < a.block_size; c0 += 32) {
+        for (int c0 = 0; c0 < limit; c0 += 32) {
             const int j = c0 + lane;
-            int nb = j < a.block_size ? __ldg(arow + j) : -1;
+            int nb = -1;
+            if (j < limit) {
+                nb = seeding ? (int)((unsigned long long)j * (unsigned long long)a.n /
+                                     (unsigned long long)a.n_multiprobe)
+                             : __ldg(arow + j);
+            }
             if (nb >= a.n) {  // impossible for a validated graph; never read out of range
                 atomicExch(a.err, 1);
                 nb = -1;
             }
-            tr.neighbor_slots_scanned += min(32, a.block_size - c0);
             const unsigned N = bloom_chunk(bloom, nb, bc, lane);
-            const float d = dist(nb, N);
+            float d;
+            if constexpr (KIND == 0) {
+                const float* base = reinterpret_cast<const float*>(a.base);
+                if constexpr (kIntPath) {
+                    if (int_exact) d = l2_int<NE>(base, a.ld, qv, nb, N, rows, lane);
+                    else d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
+                } else {
+                    d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
+                }
+            } else {
+                d = ham_lane<NE>(reinterpret_cast<const uint32_t*>(a.base), a.ld, qcode, nb,
+                                 (N >> lane) & 1u);
+            }
             const int c = __popc(N);
+            if (seeding) {
+                tr.seed_count += c;
+            } else {
+                tr.neighbor_slots_scanned += min(32, limit - c0);
+                tr.candidate_nodes += c;
+            }
             tr.visited_nodes += c;
-            tr.candidate_nodes += c;
             tr.distance_evals += c;
-            tr.frontier_pushes += q_push(cand, N, d, nb, lane);
-            tr.result_updates += q_push(res, N, d, nb, lane);
+            tr.frontier_pushes += q_push<true>(cand, N, d, nb, lane);
+            tr.result_updates += q_push<false>(res, N, d, nb, lane);
             if (N) {
                 tr.peak_frontier = max(tr.peak_frontier, cand.sz);
                 tr.peak_results = max(tr.peak_results, res.sz);
             }
         }
+        seeding = false;
     }
 
-    // Trim to k (Results::pop_worst), then k x drain_best (kernalGraph.h:292-296).
-    while (res.sz > a.k) {
-        q_argmax(res, lane);
-        if (lane == 0) {
-            res.d[res.maxi] = res.d[res.sz - 1];
-            res.id[res.maxi] = res.id[res.sz - 1];
-        }
-        res.sz -= 1;
-        __syncwarp();
-    }
-    const int cnt = res.sz < a.k ? res.sz : a.k;
-    int32_t* out = a.out + (int64_t)qid * a.k;
-    for (int i = 0; i < cnt; ++i) {
-        float v;
-        int m;
-        q_argmin(res, lane, v, m);
-        const int id = res.id[m];
-        __syncwarp();
-        if (lane == 0) {
-            out[i] = id;
-            res.d[m] = res.d[res.sz - 1];
-            res.id[m] = res.id[res.sz - 1];
-        }
-        res.sz -= 1;
-        __syncwarp();
-    }
-    for (int i = cnt + lane; i < a.k; i += 32) out[i] = -1;
-    tr.result_count = cnt;
+    tr.result_count = finish(res, cand, a.k, a.out + (int64_t)qid * a.k, lane);
     if (a.trace != nullptr && lane == 0) a.trace[qid] = tr;
 }
 
-template <int KIND, int NE>
+template <int KIND, int NE, int GPL>
 __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -464,42 +644,55 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         if (lane == 0) qid = (int)atomicAdd(a.counter, 1u);
         qid = __shfl_sync(FULL, qid, 0);
         if (qid >= a.nq) break;
-        search_query<KIND, NE>(a, qid, ws, lane);
+        search_query<KIND, NE, GPL>(a, qid, ws, lane);
     }
 }
 
 using KernelFn = void (*)(const SearchArgs);
 
-KernelFn pick_kernel(int kind, const SearchArgs& a) {
+template <int GPL>
+KernelFn pick_gpl(int kind, const SearchArgs& a) {
     if (kind == SONG_KIND_L2) {
-        if (a.dim <= 32) return search_kernel<0, 1>;
-        if (a.dim <= 64) return search_kernel<0, 2>;
-        if (a.dim <= 128) return search_kernel<0, 4>;
-        if (a.dim <= 256) return search_kernel<0, 8>;
-        return search_kernel<0, 0>;
+        if (a.dim <= 32) return search_kernel<0, 1, GPL>;
+        if (a.dim <= 64) return search_kernel<0, 2, GPL>;
+        if (a.dim <= 128) return search_kernel<0, 4, GPL>;
+        if (a.dim <= 256) return search_kernel<0, 8, GPL>;
+        return search_kernel<0, 0, GPL>;
     }
-    switch (a.ld / 4) {
-        case 1: return search_kernel<1, 1>;
-        case 2: return search_kernel<1, 2>;
-        case 3: return search_kernel<1, 3>;
-        case 4: return search_kernel<1, 4>;
-        case 5: return search_kernel<1, 5>;
-        case 6: return search_kernel<1, 6>;
-        case 7: return search_kernel<1, 7>;
-        case 8: return search_kernel<1, 8>;
+    switch (a.ld) {
+        case 4: return search_kernel<1, 1, GPL>;
+        case 8: return search_kernel<1, 2, GPL>;
+        case 16: return search_kernel<1, 4, GPL>;
+        case 32: return search_kernel<1, 8, GPL>;
         default: return nullptr;
     }
+}
+
+KernelFn pick_kernel(int kind, const SearchArgs& a) {
+    if (a.cap <= 1024) return pick_gpl<1>(kind, a);
+    if (a.cap <= 2048) return pick_gpl<2>(kind, a);
+    if (a.cap <= 4096) return pick_gpl<4>(kind, a);
+    return nullptr;
 }
 
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 }  // namespace
 
+int search_row_stride(int kind, int dim) {
+    if (kind == SONG_KIND_L2) return round_up(dim, 4);
+    if (dim <= 4) return 4;
+    if (dim <= 8) return 8;
+    if (dim <= 16) return 16;
+    return 32;
+}
+
 int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a) {
     (void)kind;
-    const int capr = round_up(cap, 4);
+    const int capr = round_up(cap, 32);
     a->q_off = 0;
-    a->cd_off = round_up(dim * 4, 16);
+    a->rows_off = round_up(dim * 4, 16);
+    a->cd_off = a->rows_off + 128;
     a->ci_off = a->cd_off + capr * 4;
     a->rd_off = a->ci_off + capr * 4;
     a->ri_off = a->rd_off + capr * 4;
