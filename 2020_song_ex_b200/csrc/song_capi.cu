@@ -76,8 +76,6 @@ song_status cuda_fail(cudaError_t e, const char* what) {
         if (_e != cudaSuccess) return cuda_fail(_e, what); \
     } while (0)
 
-int round_up4(int x) { return (x + 3) / 4 * 4; }
-
 // Each launch takes the next work counter of a ring, so launches that
 // overlap on different streams do not share one; a counter is reused after
 // kCounterRing launches on the same index.

@@ -564,6 +564,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     for (;;) {
         int limit;
         const int32_t* arow = nullptr;
+        int first = -1;  // first chunk of the adjacency row
         if (seeding) {
             limit = a.n_multiprobe;  // seeds p*n/N_MULTIPROBE (kernalGraph.h:214-231)
         } else {                     // expansion (kernalGraph.h:233-289)
@@ -572,7 +573,10 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             root_min(cand, mb, mi);
             const float cmin = __uint_as_float(mb);
             const int cn = cand.id[mi];
+            limit = a.block_size;
+            arow = a.adj + (int64_t)cn * a.block_size;
             q_remove<true>(cand, (int)mi, lane);
+            if (lane < limit) first = __ldg(arow + lane);
             tr.expanded_nodes += 1;
             if (res.sz == res.cap) {  // early stop: full and strictly worse than the worst
                 unsigned wb, wi;
@@ -582,8 +586,14 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     break;
                 }
             }
-            limit = a.block_size;
-            arow = a.adj + (int64_t)cn * a.block_size;
+            if (cand.sz > 0) {  // the next pop is most often today's runner-up: warm its row in L2
+                unsigned nb2, ni2;
+                root_min(cand, nb2, ni2);
+                if (lane == 0) {
+                    const int32_t* nrow = a.adj + (int64_t)cand.id[ni2] * a.block_size;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(nrow));
+                }
+            }
         }
         for (int c0 = 0; c0 < limit; c0 += 32) {
             const int j = c0 + lane;
@@ -591,7 +601,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             if (j < limit) {
                 nb = seeding ? (int)((unsigned long long)j * (unsigned long long)a.n /
                                      (unsigned long long)a.n_multiprobe)
-                             : __ldg(arow + j);
+                             : (c0 == 0 ? first : __ldg(arow + j));
             }
             if (nb >= a.n) {  // impossible for a validated graph; never read out of range
                 atomicExch(a.err, 1);
