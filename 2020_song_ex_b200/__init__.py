@@ -36,6 +36,9 @@ SONG_ERR_BUDGET = 5
 SONG_ERR_UNSUPPORTED = 6
 KIND_L2 = 0
 KIND_HAMMING = 1
+PREC_FP32 = 0
+PREC_BF16 = 1
+PREC_FP8 = 2
 
 TRACE_FIELDS = (
     "seed_count", "visited_nodes", "expanded_nodes", "neighbor_slots_scanned",
@@ -62,6 +65,25 @@ class _Timing(C.Structure):
     _fields_ = [("alloc_ms", C.c_double), ("h2d_ms", C.c_double), ("memset_ms", C.c_double),
                 ("kernel_ms", C.c_double), ("d2h_ms", C.c_double), ("total_ms", C.c_double),
                 ("ef_search", C.c_int), ("batch_limit", C.c_int), ("n_batches", C.c_int)]
+
+
+class _Opts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("rerank", C.c_int), ("learned", C.c_int),
+                ("stop_threshold", C.c_float), ("reserved", C.c_int * 4)]
+
+
+@dataclass
+class SearchOpts:
+    """Extended search options (song_search_opts): precision form, FP32
+    re-rank, learned entry/stop model.  The defaults select the plain search."""
+    precision: int = PREC_FP32
+    rerank: bool = False
+    learned: bool = False
+    stop_threshold: float = 0.5
+
+    def _c(self) -> _Opts:
+        return _Opts(int(self.precision), int(bool(self.rerank)), int(bool(self.learned)),
+                     float(self.stop_threshold))
 
 
 _lib: Optional[C.CDLL] = None
@@ -93,6 +115,13 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_kernel_launch_count.restype = C.c_int64
     L.song_build_graph.argtypes = [ci, vp, i64, ci, C.POINTER(_Params), ci, ci, vp]
     L.song_build_graph.restype = C.c_int
+    L.song_index_set_precision.argtypes = [vp, ci]
+    L.song_index_set_precision.restype = C.c_int
+    L.song_search_device_ex.argtypes = [vp, C.POINTER(_Opts), vp, ci, ci, ci, vp, vp, vp, vp]
+    L.song_search_device_ex.restype = C.c_int
+    L.song_gpu_search_ex.argtypes = [vp, C.POINTER(_Opts), vp, ci, ci, ci, ci, vp, vp, vp,
+                                     C.POINTER(_Timing)]
+    L.song_gpu_search_ex.restype = C.c_int
     for name in ("song_index_create_l2", "song_index_create_hamming", "song_index_destroy",
                  "song_index_info", "song_gpu_search", "song_gpu_search_hamming",
                  "song_search_device"):
@@ -321,3 +350,45 @@ def search_device(g, d_queries, nq: int, k: int, ef_search: int, d_ids, d_traces
         st = int(getattr(stream, "cuda_stream", stream))
     _check(load_library().song_search_device(g._h, ptr(d_queries), nq, k, ef_search, ptr(d_ids),
                                              ptr(d_traces), st))
+
+
+def set_precision(g: KernelGraph, precision: int) -> None:
+    """Attach a BF16 or FP8 (per-vector scale) copy of the rows for the precision form."""
+    _check(load_library().song_index_set_precision(g._h, int(precision)))
+
+
+def search_device_ex(g, opts: Optional[SearchOpts], d_queries, nq: int, k: int, ef_search: int,
+                     d_ids, d_dists=None, d_traces=None, stream=None) -> None:
+    """song_search_device_ex on device pointers / torch CUDA tensors (asynchronous)."""
+    def ptr(x):
+        if x is None:
+            return None
+        return int(x.data_ptr()) if hasattr(x, "data_ptr") else int(x)
+    st = None
+    if stream is not None:
+        st = int(getattr(stream, "cuda_stream", stream))
+    o = (opts or SearchOpts())._c()
+    _check(load_library().song_search_device_ex(g._h, C.byref(o), ptr(d_queries), nq, k,
+                                                ef_search, ptr(d_ids), ptr(d_dists),
+                                                ptr(d_traces), st))
+
+
+def gpu_search_ex(g, opts: Optional[SearchOpts], queries, nq: int, k: int,
+                  ef_search: Optional[int] = None, N_MULTIQUERY: int = 512,
+                  trace: Optional[GpuSearchTrace] = None):
+    """Host-buffer extended search; returns (ids [nq, k], dists [nq, k])."""
+    L = load_library()
+    ef = g.params.pq_size if ef_search is None else int(ef_search)
+    q = np.ascontiguousarray(np.asarray(queries, dtype=np.float32).reshape(nq, -1))
+    ids = np.empty((nq, max(k, 1)), dtype=np.int32)
+    dists = np.empty((nq, max(k, 1)), dtype=np.float32)
+    tq = np.zeros((nq, 12), dtype=np.int32) if trace is not None else None
+    t = _Timing()
+    o = (opts or SearchOpts())._c()
+    _check(L.song_gpu_search_ex(g._h, C.byref(o), q.ctypes.data, nq, k, N_MULTIQUERY, ef,
+                                ids.ctypes.data, dists.ctypes.data,
+                                tq.ctypes.data if tq is not None else None, C.byref(t)))
+    if trace is not None:
+        trace.ef_search, trace.kernel_ms, trace.total_ms = t.ef_search, t.kernel_ms, t.total_ms
+        trace.queries = tq
+    return ids[:, :k], dists[:, :k]

@@ -51,6 +51,14 @@ struct song_index {
     size_t ids_cap = 0;
     song_query_trace* d_tr = nullptr;
     size_t tr_cap = 0;
+    float* d_dist = nullptr;
+    size_t dist_cap = 0;
+    // precision form: compressed copies of the FP32 rows
+    void* d_bf16 = nullptr;
+    int bf16_ld = 0;  // bytes per row
+    void* d_fp8 = nullptr;
+    float* d_fp8_scale = nullptr;
+    int fp8_ld = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
@@ -120,6 +128,10 @@ void free_index(song_index* x) {
     cudaFree(x->d_q);
     cudaFree(x->d_ids);
     cudaFree(x->d_tr);
+    cudaFree(x->d_dist);
+    cudaFree(x->d_bf16);
+    cudaFree(x->d_fp8);
+    cudaFree(x->d_fp8_scale);
     if (x->ev0) cudaEventDestroy(x->ev0);
     if (x->ev1) cudaEventDestroy(x->ev1);
     if (x->stream) cudaStreamDestroy(x->stream);
@@ -195,7 +207,8 @@ int clamp_ef(int ef, int k, int pq_size) {  // kernalGraph.h:315-316
 
 // Fill SearchArgs for one launch over `nq` queries at d_q / d_ids / d_tr.
 song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int32_t* d_ids,
-                      song_query_trace* d_tr, song::SearchArgs* a) {
+                      song_query_trace* d_tr, song::SearchArgs* a,
+                      const song_search_opts* opts = nullptr, float* d_dist = nullptr) {
     const int cap = ef < 1 ? 1 : (ef > x->p.pq_size ? x->p.pq_size : ef);  // Candidates::init
     std::memset(a, 0, sizeof *a);
     a->base = x->d_base;
@@ -219,7 +232,26 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
     a->int_base = x->range.int_base;
     a->base_min = x->range.lo;
     a->base_max = x->range.hi;
-    song::search_warp_smem(x->kind, x->dim, cap, x->p.bf_words, a);
+    a->out_dist = d_dist;
+    a->qdim = x->dim;
+    const int prec = opts ? opts->precision : SONG_PREC_FP32;
+    if (prec != SONG_PREC_FP32) {
+        if (x->kind != SONG_KIND_L2)
+            return fail(SONG_ERR_UNSUPPORTED, "the precision form applies to L2 indexes");
+        if (prec == SONG_PREC_BF16 && x->d_bf16 == nullptr)
+            return fail(SONG_ERR_INVALID_ARG, "BF16 rows not attached (song_index_set_precision)");
+        if (prec == SONG_PREC_FP8 && x->d_fp8 == nullptr)
+            return fail(SONG_ERR_INVALID_ARG, "FP8 rows not attached (song_index_set_precision)");
+        if (prec != SONG_PREC_BF16 && prec != SONG_PREC_FP8)
+            return fail(SONG_ERR_INVALID_ARG, "unknown precision");
+        a->prec = prec;
+        a->lowp = prec == SONG_PREC_BF16 ? x->d_bf16 : x->d_fp8;
+        a->scales = x->d_fp8_scale;
+        a->lowp_ld = prec == SONG_PREC_BF16 ? x->bf16_ld : x->fp8_ld;
+        a->qdim = song::lowp_padded_dim(prec, x->dim);
+        a->rerank = opts->rerank ? 1 : 0;
+    }
+    song::search_warp_smem(x->kind, a->qdim, cap, x->p.bf_words, a);
     if (cap > 4096)
         return fail(SONG_ERR_UNSUPPORTED, "queue capacity above 4096 slots (pq_size and ef) is not supported");
     int optin = 0;
@@ -246,7 +278,8 @@ song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
 
 song_status host_search(song_index* x, int kind, const void* queries, int nq, int k,
                         int n_multiquery, int ef_search, int32_t* ids, song_query_trace* traces,
-                        song_timing* timing) {
+                        song_timing* timing, const song_search_opts* opts = nullptr,
+                        float* dists = nullptr) {
     using clk = std::chrono::high_resolution_clock;
     auto ms = [](clk::time_point a, clk::time_point b) {
         return std::chrono::duration<double, std::milli>(b - a).count();
@@ -275,6 +308,9 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
         SONG_CUDA(grow(&x->d_tr, &x->tr_cap,
                        std::max<size_t>(48, (size_t)std::min(nq, chunk) * sizeof(song_query_trace))),
                   "trace staging alloc");
+    if (dists)
+        SONG_CUDA(grow(&x->d_dist, &x->dist_cap, std::max<size_t>(4, (size_t)std::min(nq, chunk) * k * 4)),
+                  "distance staging alloc");
     auto t1 = clk::now();
     t.alloc_ms = ms(t0, t1);
     cudaStream_t st = x->stream;
@@ -287,7 +323,8 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
         SONG_CUDA(cudaStreamSynchronize(st), "query H2D sync");
         auto b1 = clk::now();
         song::SearchArgs a;
-        if (song_status s = make_args(x, x->d_q, bs, k, ef, x->d_ids, traces ? x->d_tr : nullptr, &a))
+        if (song_status s = make_args(x, x->d_q, bs, k, ef, x->d_ids, traces ? x->d_tr : nullptr, &a,
+                                      opts, dists ? x->d_dist : nullptr))
             return s;
         SONG_CUDA(cudaEventRecord(x->ev0, st), "event");
         if (song_status s = launch(x, a, st)) return s;
@@ -304,6 +341,10 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
             SONG_CUDA(cudaMemcpyAsync(traces + off, x->d_tr, (size_t)bs * sizeof(song_query_trace),
                                       cudaMemcpyDeviceToHost, st),
                       "trace D2H");
+        if (dists && k > 0)
+            SONG_CUDA(cudaMemcpyAsync(dists + (size_t)off * k, x->d_dist, (size_t)bs * k * 4,
+                                      cudaMemcpyDeviceToHost, st),
+                      "distance D2H");
         SONG_CUDA(cudaStreamSynchronize(st), "D2H sync");
         auto b3 = clk::now();
         t.h2d_ms += ms(b0, b1);
@@ -460,6 +501,58 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
     if (st) cudaStreamDestroy(st);
     if (e != cudaSuccess) return cuda_fail(e, "graph build");
     return SONG_OK;
+}
+
+song_status song_index_set_precision(song_index* x, int precision) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (x->kind != SONG_KIND_L2) return fail(SONG_ERR_UNSUPPORTED, "the precision form applies to L2 indexes");
+    if (precision != SONG_PREC_BF16 && precision != SONG_PREC_FP8)
+        return fail(SONG_ERR_INVALID_ARG, "precision must be SONG_PREC_BF16 or SONG_PREC_FP8");
+    std::lock_guard<std::mutex> lock(x->mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != x->device) SONG_CUDA(cudaSetDevice(x->device), "cudaSetDevice");
+    const int pd = song::lowp_padded_dim(precision, x->dim);
+    const int row_bytes = precision == SONG_PREC_BF16 ? pd * 2 : pd;
+    void** dst = precision == SONG_PREC_BF16 ? &x->d_bf16 : &x->d_fp8;
+    cudaFree(*dst);
+    *dst = nullptr;
+    SONG_CUDA(cudaMalloc(dst, (size_t)x->n * row_bytes), "compressed rows alloc");
+    if (precision == SONG_PREC_FP8) {
+        cudaFree(x->d_fp8_scale);
+        x->d_fp8_scale = nullptr;
+        SONG_CUDA(cudaMalloc(&x->d_fp8_scale, (size_t)x->n * sizeof(float)), "scale alloc");
+    }
+    SONG_CUDA(song::quantize_rows(precision, (const float*)x->d_base, x->n, x->dim, x->ld, *dst,
+                                  row_bytes, x->d_fp8_scale, x->stream),
+              "quantize");
+    SONG_CUDA(cudaStreamSynchronize(x->stream), "quantize sync");
+    if (precision == SONG_PREC_BF16) x->bf16_ld = row_bytes; else x->fp8_ld = row_bytes;
+    return SONG_OK;
+}
+
+song_status song_search_device_ex(song_index* x, const song_search_opts* opts,
+                                  const void* d_queries, int nq, int k, int ef_search,
+                                  int32_t* d_ids, float* d_dists, song_query_trace* d_traces,
+                                  void* stream) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (nq < 0 || k < 0) return fail(SONG_ERR_INVALID_ARG, "nq and k must be >= 0");
+    if (nq == 0) return SONG_OK;
+    if (d_queries == nullptr || (k > 0 && d_ids == nullptr))
+        return fail(SONG_ERR_INVALID_ARG, "queries or ids is NULL");
+    const int ef = clamp_ef(ef_search, k, x->p.pq_size);
+    std::lock_guard<std::mutex> lock(x->mu);
+    song::SearchArgs a;
+    if (song_status s = make_args(x, d_queries, nq, k, ef, d_ids, d_traces, &a, opts, d_dists)) return s;
+    return launch(x, a, (cudaStream_t)stream);
+}
+
+song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,
+                               const float* queries, int nq, int k, int n_multiquery,
+                               int ef_search, int32_t* ids, float* dists,
+                               song_query_trace* traces, song_timing* timing) {
+    return host_search(index, index ? index->kind : SONG_KIND_L2, queries, nq, k, n_multiquery,
+                       ef_search, ids, traces, timing, opts, dists);
 }
 
 int64_t song_kernel_launch_count(void) { return song::g_launches.load(); }

@@ -31,7 +31,24 @@ struct SearchArgs {
     int q_off, rows_off, cd_off, ci_off, rd_off, ri_off, bl_off;  // per-warp carve-up, bytes
     int int_base;            // 1: every base value is an integer in [base_min, base_max]
     float base_min, base_max;
+    // precision form (prec != SONG_PREC_FP32)
+    int prec;                // SONG_PREC_FP32 / SONG_PREC_BF16 / SONG_PREC_FP8
+    const void* lowp;        // compressed rows [n x lowp_ld bytes]
+    const float* scales;     // FP8: per-vector scale [n]
+    int lowp_ld;             // bytes per compressed row (multiple of 128)
+    int qdim;                // floats of the query kept in shared memory (padded dim)
+    int rerank;              // 1: exact FP32 re-rank of the final results queue
+    float* out_dist;         // [nq x k] distance of each output id (nullable)
 };
+
+// Padded element count of a compressed row (a whole number of 128-byte
+// lines per 8-lane group) and its byte stride.
+int lowp_padded_dim(int prec, int dim);
+
+// Fill the compressed copy of the FP32 rows: BF16 (round to nearest even) or
+// FP8 e4m3 with a per-vector scale amax/448.  Stream-ordered.
+cudaError_t quantize_rows(int prec, const float* d_rows, int64_t n, int dim, int ld, void* d_out,
+                          int out_ld, float* d_scales, cudaStream_t st);
 
 // Integer range of FP32 rows (0 in int_base if any value is not an integer).
 struct BaseRange {
@@ -43,7 +60,7 @@ BaseRange scan_base_range(const float* rows, int64_t n, int dim);
 // Row stride (elements) the kernels use for `dim` elements of `kind`.
 int search_row_stride(int kind, int dim);
 
-// Per-warp shared-memory layout for (kind, dim, cap, bf_words).
+// Per-warp shared-memory layout for (kind, query floats, cap, bf_words).
 int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a);
 
 // Launch the plain search on `stream`: chooses the kernel instance for

@@ -34,6 +34,10 @@
 //  * The final trim (pop_worst) and drain (drain_best) are replayed exactly;
 //    when the k+1 smallest results have distinct distances their outcome is
 //    simply those k in ascending order, which is taken directly.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
+
 #include <algorithm>
 #include <atomic>
 #include <climits>
@@ -437,7 +441,7 @@ __device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int
 // Otherwise the extraction is undone and the trims and drains are replayed.
 template <int GPL>
 __device__ __forceinline__ int finish(Queue<GPL>& res, Queue<GPL>& cand, int k, int32_t* out,
-                                      int lane) {
+                                      float* outd, int lane) {
     const int ng = (res.sz + 31) >> 5;
     for (int g = 0; g < ng; ++g) group_update<true>(res, g, lane);
     const int cnt = res.sz < k ? res.sz : k;
@@ -459,7 +463,10 @@ __device__ __forceinline__ int finish(Queue<GPL>& res, Queue<GPL>& cand, int k, 
     for (int i = lane; i + 1 < take; i += 32) distinct &= xv[i] < xv[i + 1];
     distinct = __all_sync(FULL, distinct);
     if (distinct) {
-        for (int i = lane; i < cnt; i += 32) out[i] = res.id[xs[i]];
+        for (int i = lane; i < cnt; i += 32) {
+            out[i] = res.id[xs[i]];
+            if (outd) outd[i] = __uint_as_float(xv[i]);
+        }
     } else {
         for (int i = lane; i < take; i += 32) reinterpret_cast<unsigned*>(res.d)[xs[i]] = xv[i];
         __syncwarp();
@@ -473,17 +480,178 @@ __device__ __forceinline__ int finish(Queue<GPL>& res, Queue<GPL>& cand, int k, 
             unsigned mb, mi;
             root_min(res, mb, mi);
             const int id = res.id[mi];
-            if (lane == 0) out[i] = id;
+            if (lane == 0) {
+                out[i] = id;
+                if (outd) outd[i] = __uint_as_float(mb);
+            }
             q_remove<true>(res, (int)mi, lane);
         }
     }
-    for (int i = cnt + lane; i < k; i += 32) out[i] = -1;
+    for (int i = cnt + lane; i < k; i += 32) {
+        out[i] = -1;
+        if (outd) outd[i] = INFINITY;
+    }
+    return cnt;
+}
+
+// Accumulate (q - b)^2 over one 16-byte chunk of a compressed row: 8 BF16 or
+// 16 FP8 e4m3 values (times the row's scale), FP32 arithmetic.
+template <int DT>
+__device__ __forceinline__ void chunk_l2(const uint4 x, const float* qc, float scale, float& acc) {
+    const unsigned w[4] = {x.x, x.y, x.z, x.w};
+    if constexpr (DT == SONG_PREC_BF16) {
+        const float4 q0 = *reinterpret_cast<const float4*>(qc);
+        const float4 q1 = *reinterpret_cast<const float4*>(qc + 4);
+        const float q[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float lo = __uint_as_float(w[i] << 16);
+            const float hi = __uint_as_float(w[i] & 0xffff0000u);
+            float t = q[2 * i] - lo;
+            acc = fmaf(t, t, acc);
+            t = q[2 * i + 1] - hi;
+            acc = fmaf(t, t, acc);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float4 q = *reinterpret_cast<const float4*>(qc + 4 * i);
+            const __half2_raw h01 = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] & 0xffffu), __NV_E4M3);
+            const __half2_raw h23 = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] >> 16), __NV_E4M3);
+            const float2 b01 = __half22float2(__half2(h01));
+            const float2 b23 = __half22float2(__half2(h23));
+            float t = fmaf(-scale, b01.x, q.x);
+            acc = fmaf(t, t, acc);
+            t = fmaf(-scale, b01.y, q.y);
+            acc = fmaf(t, t, acc);
+            t = fmaf(-scale, b23.x, q.z);
+            acc = fmaf(t, t, acc);
+            t = fmaf(-scale, b23.y, q.w);
+            acc = fmaf(t, t, acc);
+        }
+    }
+}
+
+// Precision-form distances of the rows of the lanes in N (lane j gets its
+// own row's): 4 rows per pass, 8 lanes per row, 16-byte loads of the
+// compressed rows, query from shared memory, two passes in flight.
+template <int DT>
+__device__ __forceinline__ float l2_lowp(const SearchArgs& a, const float* sq, int nb, unsigned N,
+                                         int* rows, int lane) {
+    constexpr int EPC = DT == SONG_PREC_BF16 ? 8 : 16;  // elements per 16-byte chunk
+    const bool mine = (N >> lane) & 1u;
+    const int rank = __popc(N & lanemask_lt(lane));
+    const int m = __popc(N);
+    if (mine) rows[rank] = nb;
+    __syncwarp();
+    const int grp = lane >> 3, t = lane & 7;
+    const int nchunk = a.lowp_ld >> 4;
+    const unsigned char* lp = reinterpret_cast<const unsigned char*>(a.lowp);
+    float out = 0.0f;
+    for (int p0 = 0; p0 < m; p0 += 8) {
+        const int ra = p0 + grp, rb = p0 + 4 + grp;
+        const bool va = ra < m, vb = rb < m;
+        const int ia = va ? rows[ra] : 0, ib = vb ? rows[rb] : 0;
+        const uint4* pa = reinterpret_cast<const uint4*>(lp + (size_t)ia * a.lowp_ld);
+        const uint4* pb = reinterpret_cast<const uint4*>(lp + (size_t)ib * a.lowp_ld);
+        float sca = 1.0f, scb = 1.0f;
+        if constexpr (DT == SONG_PREC_FP8) {
+            sca = va ? __ldg(a.scales + ia) : 0.0f;
+            scb = vb ? __ldg(a.scales + ib) : 0.0f;
+        }
+        float sa = 0.0f, sb = 0.0f;
+        for (int c = t; c < nchunk; c += 8) {
+            const uint4 xa = va ? __ldg(pa + c) : make_uint4(0u, 0u, 0u, 0u);
+            const uint4 xb = vb ? __ldg(pb + c) : make_uint4(0u, 0u, 0u, 0u);
+            chunk_l2<DT>(xa, sq + c * EPC, sca, sa);
+            chunk_l2<DT>(xb, sq + c * EPC, scb, sb);
+        }
+#pragma unroll
+        for (int w = 4; w >= 1; w >>= 1) {
+            sa += __shfl_xor_sync(FULL, sa, w);
+            sb += __shfl_xor_sync(FULL, sb, w);
+        }
+        const float ga = __shfl_sync(FULL, sa, (rank & 3) << 3);
+        const float gb = __shfl_sync(FULL, sb, (rank & 3) << 3);
+        if (mine && (rank >> 2) == (p0 >> 2)) out = ga;
+        if (mine && (rank >> 2) == (p0 >> 2) + 1) out = gb;
+    }
+    __syncwarp();
+    return out;
+}
+
+// Precision form, final step: exact FP32 distances of every entry of the
+// results queue (FP32 rows, 8 lanes per row), then the k smallest by
+// (distance, id) in ascending order, -1 padded.
+template <int GPL>
+__device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL>& res,
+                                             Queue<GPL>& cand, const float* sq, int32_t* out,
+                                             float* outd, int lane) {
+    const int m = res.sz;
+    float* rd = cand.d;
+    int* rid = cand.id;
+    const float* base = reinterpret_cast<const float*>(a.base);
+    const int nch = a.ld >> 2;  // float4 per FP32 row
+    const int grp = lane >> 3, t = lane & 7;
+    for (int p0 = 0; p0 < m; p0 += 4) {
+        const int r = p0 + grp;
+        const bool v = r < m;
+        const int id = v ? res.id[r] : 0;
+        const float4* row = reinterpret_cast<const float4*>(base + (size_t)id * a.ld);
+        float acc = 0.0f;
+        for (int c = t; c < nch; c += 8) {
+            const float4 x = v ? __ldg(row + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 q = *reinterpret_cast<const float4*>(sq + 4 * c);
+            float u = q.x - x.x;
+            acc = fmaf(u, u, acc);
+            u = q.y - x.y;
+            acc = fmaf(u, u, acc);
+            u = q.z - x.z;
+            acc = fmaf(u, u, acc);
+            u = q.w - x.w;
+            acc = fmaf(u, u, acc);
+        }
+#pragma unroll
+        for (int w = 4; w >= 1; w >>= 1) acc += __shfl_xor_sync(FULL, acc, w);
+        if (t == 0 && v) {
+            rd[r] = acc;
+            rid[r] = id;
+        }
+    }
+    __syncwarp();
+    const int cnt = m < a.k ? m : a.k;
+    for (int i = 0; i < cnt; ++i) {
+        unsigned bb = 0xffffffffu, bi = 0xffffffffu;
+        for (int s2 = lane; s2 < m; s2 += 32) {
+            const unsigned b = fbits(rd[s2]);
+            const unsigned id = (unsigned)rid[s2];
+            if (b < bb || (b == bb && id < bi)) {
+                bb = b;
+                bi = id;
+            }
+        }
+        const unsigned mb = __reduce_min_sync(FULL, bb);
+        const unsigned mi = __reduce_min_sync(FULL, bb == mb ? bi : 0xffffffffu);
+        if (lane == 0) {
+            out[i] = (int)mi;
+            if (outd) outd[i] = __uint_as_float(mb);
+        }
+        for (int s2 = lane; s2 < m; s2 += 32)  // taken: out of every later minimum
+            if ((unsigned)rid[s2] == mi) rd[s2] = __uint_as_float(0xffffffffu);
+        __syncwarp();
+    }
+    for (int i = cnt + lane; i < a.k; i += 32) {
+        out[i] = -1;
+        if (outd) outd[i] = INFINITY;
+    }
     return cnt;
 }
 
 // KIND 0 = L2 with NE query elements per lane (0: query in shared memory);
 // KIND 1 = Hamming with NE uint4 of code per row.  GPL: queue groups per lane.
-template <int KIND, int NE, int GPL>
+// DT: SONG_PREC_FP32 (the plain, bit-exact search) or the precision form on
+// BF16 / FP8 rows (KIND 0, query in shared memory, FP32 re-rank at the end).
+template <int KIND, int NE, int GPL, int DT>
 __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsigned char* ws,
                                              int lane) {
     Queue<GPL> cand, res;
@@ -501,7 +669,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     bc.nhash = a.bf_nhash;
 
     // Query in registers (and shared memory for the generic L2 path).
-    constexpr bool kIntPath = KIND == 0 && NE > 0;
+    constexpr bool kIntPath = KIND == 0 && NE > 0 && DT == SONG_PREC_FP32;
     float qreg[(KIND == 0 && NE > 0) ? NE : 1];
     float4 qv[kIntPath ? NE : 1];
     uint4 qcode[KIND == 1 ? NE : 1];
@@ -544,7 +712,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             }
         } else {
             qreg[0] = 0.0f;
-            for (int i = lane; i < a.dim; i += 32) sq[i] = qg[i];
+            for (int i = lane; i < a.qdim; i += 32) sq[i] = i < a.dim ? qg[i] : 0.0f;
         }
     } else {
         const uint32_t* qg = reinterpret_cast<const uint32_t*>(a.queries) + (int64_t)qid * a.qld;
@@ -609,7 +777,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             }
             const unsigned N = bloom_chunk(bloom, nb, bc, lane);
             float d;
-            if constexpr (KIND == 0) {
+            if constexpr (DT != SONG_PREC_FP32) {
+                d = l2_lowp<DT>(a, sq, nb, N, rows, lane);
+            } else if constexpr (KIND == 0) {
                 const float* base = reinterpret_cast<const float*>(a.base);
                 if constexpr (kIntPath) {
                     if (int_exact) d = l2_int<NE>(base, a.ld, qv, nb, N, rows, lane);
@@ -640,11 +810,15 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         seeding = false;
     }
 
-    tr.result_count = finish(res, cand, a.k, a.out + (int64_t)qid * a.k, lane);
+    float* outd = a.out_dist ? a.out_dist + (int64_t)qid * a.k : nullptr;
+    if (DT != SONG_PREC_FP32 && a.rerank)
+        tr.result_count = rerank_finish(a, res, cand, sq, a.out + (int64_t)qid * a.k, outd, lane);
+    else
+        tr.result_count = finish(res, cand, a.k, a.out + (int64_t)qid * a.k, outd, lane);
     if (a.trace != nullptr && lane == 0) a.trace[qid] = tr;
 }
 
-template <int KIND, int NE, int GPL>
+template <int KIND, int NE, int GPL, int DT>
 __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -654,7 +828,7 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         if (lane == 0) qid = (int)atomicAdd(a.counter, 1u);
         qid = __shfl_sync(FULL, qid, 0);
         if (qid >= a.nq) break;
-        search_query<KIND, NE, GPL>(a, qid, ws, lane);
+        search_query<KIND, NE, GPL, DT>(a, qid, ws, lane);
     }
 }
 
@@ -663,19 +837,54 @@ using KernelFn = void (*)(const SearchArgs);
 template <int GPL>
 KernelFn pick_gpl(int kind, const SearchArgs& a) {
     if (kind == SONG_KIND_L2) {
-        if (a.dim <= 32) return search_kernel<0, 1, GPL>;
-        if (a.dim <= 64) return search_kernel<0, 2, GPL>;
-        if (a.dim <= 128) return search_kernel<0, 4, GPL>;
-        if (a.dim <= 256) return search_kernel<0, 8, GPL>;
-        return search_kernel<0, 0, GPL>;
+        if (a.prec == SONG_PREC_BF16) return search_kernel<0, 0, GPL, SONG_PREC_BF16>;
+        if (a.prec == SONG_PREC_FP8) return search_kernel<0, 0, GPL, SONG_PREC_FP8>;
+        if (a.dim <= 32) return search_kernel<0, 1, GPL, 0>;
+        if (a.dim <= 64) return search_kernel<0, 2, GPL, 0>;
+        if (a.dim <= 128) return search_kernel<0, 4, GPL, 0>;
+        if (a.dim <= 256) return search_kernel<0, 8, GPL, 0>;
+        return search_kernel<0, 0, GPL, 0>;
     }
     switch (a.ld) {
-        case 4: return search_kernel<1, 1, GPL>;
-        case 8: return search_kernel<1, 2, GPL>;
-        case 16: return search_kernel<1, 4, GPL>;
-        case 32: return search_kernel<1, 8, GPL>;
+        case 4: return search_kernel<1, 1, GPL, 0>;
+        case 8: return search_kernel<1, 2, GPL, 0>;
+        case 16: return search_kernel<1, 4, GPL, 0>;
+        case 32: return search_kernel<1, 8, GPL, 0>;
         default: return nullptr;
     }
+}
+
+// FP32 -> BF16 (round to nearest even) rows, zero padded to out_ld bytes.
+__global__ void quantize_bf16(const float* __restrict__ x, int64_t n, int dim, int ld,
+                              unsigned short* __restrict__ out, int out_ld) {
+    const int64_t r = blockIdx.x;
+    if (r >= n) return;
+    const int pd = out_ld / 2;
+    for (int i = threadIdx.x; i < pd; i += blockDim.x) {
+        const float v = i < dim ? x[r * ld + i] : 0.0f;
+        out[r * pd + i] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+    }
+}
+
+// FP32 -> FP8 e4m3 rows with scale amax/448 (448 = largest finite e4m3):
+// x ~= scale * e4m3(x / scale); one warp per row.
+__global__ void quantize_fp8(const float* __restrict__ x, int64_t n, int dim, int ld,
+                             unsigned char* __restrict__ out, int out_ld,
+                             float* __restrict__ scales) {
+    const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    float amax = 0.0f;
+    for (int i = lane; i < dim; i += 32) amax = fmaxf(amax, fabsf(x[r * ld + i]));
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) amax = fmaxf(amax, __shfl_xor_sync(FULL, amax, w));
+    const float scale = amax > 0.0f ? amax / 448.0f : 1.0f;
+    const float inv = 1.0f / scale;
+    for (int i = lane; i < out_ld; i += 32) {
+        const float v = i < dim ? x[r * ld + i] * inv : 0.0f;
+        out[r * out_ld + i] = (unsigned char)__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+    }
+    if (lane == 0) scales[r] = scale;
 }
 
 KernelFn pick_kernel(int kind, const SearchArgs& a) {
@@ -695,6 +904,26 @@ int search_row_stride(int kind, int dim) {
     if (dim <= 8) return 8;
     if (dim <= 16) return 16;
     return 32;
+}
+
+int lowp_padded_dim(int prec, int dim) {
+    const int unit = prec == SONG_PREC_BF16 ? 64 : 128;  // 8 lanes x 16 B per pass over a row
+    return round_up(dim, unit);
+}
+
+cudaError_t quantize_rows(int prec, const float* d_rows, int64_t n, int dim, int ld, void* d_out,
+                          int out_ld, float* d_scales, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (prec == SONG_PREC_BF16) {
+        quantize_bf16<<<(unsigned)n, 128, 0, st>>>(d_rows, n, dim, ld,
+                                                   static_cast<unsigned short*>(d_out), out_ld);
+    } else if (prec == SONG_PREC_FP8) {
+        quantize_fp8<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(
+            d_rows, n, dim, ld, static_cast<unsigned char*>(d_out), out_ld, d_scales);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a) {

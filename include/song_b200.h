@@ -31,6 +31,11 @@ typedef int song_status;
 #define SONG_ERR_BUDGET        5  /* request exceeds a memory budget                 */
 #define SONG_ERR_UNSUPPORTED   6  /* parameters outside what the kernels implement   */
 
+/* Distance precision of a search (song_search_opts.precision). */
+#define SONG_PREC_FP32  0        /* the plain search: bit-exact with the reference             */
+#define SONG_PREC_BF16  1        /* traversal on BF16 rows, FP32 accumulation                  */
+#define SONG_PREC_FP8   2        /* traversal on FP8 e4m3 rows with a per-vector FP32 scale    */
+
 /* Index kinds. */
 #define SONG_KIND_L2       0     /* FP32 vectors, squared L2 (kernalGraph.h)          */
 #define SONG_KIND_HAMMING  1     /* packed u32 sign codes, Hamming (hashKernelGraph.h) */
@@ -83,6 +88,18 @@ typedef struct song_timing {
 } song_timing;
 
 typedef struct song_index song_index;
+
+/*
+ * Options of the extended searches (no counterpart in the reference, whose
+ * only search is the plain one).  A zeroed struct selects the plain search.
+ */
+typedef struct song_search_opts {
+    int precision;        /* SONG_PREC_*; BF16/FP8 need song_index_set_precision()      */
+    int rerank;           /* 1: re-rank the final results queue with exact FP32 distances */
+    int learned;          /* 1: use the index's learned entry/stop model                 */
+    float stop_threshold; /* learned stop: stop when P(converged) >= threshold           */
+    int reserved[4];
+} song_search_opts;
 
 /* Reference defaults of config.h:9-58. */
 void song_params_default(song_params* p);
@@ -177,6 +194,31 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
 song_status song_build_graph_noalloc(int kind, const void* d_rows, int64_t n, int dim, int ld,
                                      const song_params* params, int batch_ratio,
                                      int build_bf_words, int32_t* d_adj, void* stream);
+
+/*
+ * Attach a compressed copy of an L2 index's vectors for the precision form
+ * (SONG_PREC_BF16 or SONG_PREC_FP8), converted on the GPU from the FP32
+ * copy, which stays resident for the exact re-rank.  Replaces an earlier
+ * compressed copy.
+ */
+song_status song_index_set_precision(song_index* index, int precision);
+
+/*
+ * The extended search on device pointers: opts selects precision, FP32
+ * re-rank and the learned model; d_dists (nullable) receives the distance
+ * of every output id (the FP32 distance after a re-rank).  With a zeroed
+ * opts (or NULL) it is song_search_device plus distances.
+ */
+song_status song_search_device_ex(song_index* index, const song_search_opts* opts,
+                                  const void* d_queries, int nq, int k, int ef_search,
+                                  int32_t* d_ids, float* d_dists, song_query_trace* d_traces,
+                                  void* stream);
+
+/* The extended search with host buffers (gpu_search-style, synchronous). */
+song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,
+                               const float* queries, int nq, int k, int n_multiquery,
+                               int ef_search, int32_t* ids, float* dists,
+                               song_query_trace* traces, song_timing* timing);
 
 /* Number of search-kernel launches issued by this library since load. */
 int64_t song_kernel_launch_count(void);
