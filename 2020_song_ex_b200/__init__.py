@@ -86,6 +86,20 @@ class SearchOpts:
                      float(self.stop_threshold))
 
 
+class _LearnParams(C.Structure):
+    _fields_ = [("k", C.c_int), ("ef", C.c_int), ("ckpt_every", C.c_int),
+                ("min_expansions", C.c_int), ("max_ckpt", C.c_int), ("entry_steps", C.c_int),
+                ("stop_steps", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
+                ("seed", C.c_uint)]
+
+
+class _LearnReport(C.Structure):
+    _fields_ = [("n_hubs", C.c_int), ("stop_samples", C.c_longlong),
+                ("entry_loss_first", C.c_double), ("entry_loss_last", C.c_double),
+                ("stop_loss_first", C.c_double), ("stop_loss_last", C.c_double),
+                ("stop_pos_frac", C.c_double)]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -122,6 +136,16 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_gpu_search_ex.argtypes = [vp, C.POINTER(_Opts), vp, ci, ci, ci, ci, vp, vp, vp,
                                      C.POINTER(_Timing)]
     L.song_gpu_search_ex.restype = C.c_int
+    L.song_learn_params_default.argtypes = [C.POINTER(_LearnParams)]
+    L.song_learn_params_default.restype = None
+    L.song_index_learn.argtypes = [vp, C.POINTER(_LearnParams), vp, ci, vp, C.POINTER(_LearnReport)]
+    L.song_index_learn.restype = C.c_int
+    L.song_index_get_model.argtypes = [vp, vp, ci, C.POINTER(ci)]
+    L.song_index_get_model.restype = C.c_int
+    L.song_index_set_model.argtypes = [vp, vp, ci]
+    L.song_index_set_model.restype = C.c_int
+    L.song_mlp_grad.argtypes = [ci, ci, vp, vp, vp, vp, ci, vp, C.POINTER(C.c_double)]
+    L.song_mlp_grad.restype = C.c_int
     for name in ("song_index_create_l2", "song_index_create_hamming", "song_index_destroy",
                  "song_index_info", "song_gpu_search", "song_gpu_search_hamming",
                  "song_search_device"):
@@ -392,3 +416,67 @@ def gpu_search_ex(g, opts: Optional[SearchOpts], queries, nq: int, k: int,
         trace.ef_search, trace.kernel_ms, trace.total_ms = t.ef_search, t.kernel_ms, t.total_ms
         trace.queries = tq
     return ids[:, :k], dists[:, :k]
+
+
+@dataclass
+class LearnParams:
+    """song_learn_params: traces come from the plain search at (k, ef)."""
+    k: int = 10
+    ef: int = 128
+    ckpt_every: int = 4
+    min_expansions: int = 8
+    max_ckpt: int = 256
+    entry_steps: int = 1500
+    stop_steps: int = 3000
+    batch: int = 4096
+    lr: float = 2e-3
+    seed: int = 2020
+
+    def _c(self) -> _LearnParams:
+        return _LearnParams(self.k, self.ef, self.ckpt_every, self.min_expansions, self.max_ckpt,
+                            self.entry_steps, self.stop_steps, self.batch, float(self.lr),
+                            int(self.seed))
+
+
+def learn(g: KernelGraph, d_train_queries, nq: int, d_train_nn1,
+          params: Optional[LearnParams] = None) -> dict:
+    """Train the entry and stop models on the GPU (song_index_learn).
+
+    ``d_train_queries`` [nq, dim] FP32 and ``d_train_nn1`` [nq] int32 (the
+    exact nearest neighbour of each training query) are device tensors.
+    """
+    p = (params or LearnParams())._c()
+    rep = _LearnReport()
+    _check(load_library().song_index_learn(g._h, C.byref(p), int(d_train_queries.data_ptr()), nq,
+                                           int(d_train_nn1.data_ptr()), C.byref(rep)))
+    return {f: getattr(rep, f) for f, _ in _LearnReport._fields_}
+
+
+def get_model(g: KernelGraph) -> np.ndarray:
+    """The attached learned models as a flat float32 array (save with np.save)."""
+    L = load_library()
+    n = C.c_int()
+    _check(L.song_index_get_model(g._h, None, 0, C.byref(n)))
+    blob = np.empty(n.value, dtype=np.float32)
+    _check(L.song_index_get_model(g._h, blob.ctypes.data, n.value, C.byref(n)))
+    return blob
+
+
+def set_model(g: KernelGraph, blob: np.ndarray) -> None:
+    blob = np.ascontiguousarray(blob, dtype=np.float32)
+    _check(load_library().song_index_set_model(g._h, blob.ctypes.data, blob.size))
+
+
+def mlp_grad(params: np.ndarray, out: int, loss_kind: int, x, y, w=None):
+    """Mean loss and parameter gradient of the learned-model MLP from the GPU
+    training kernels (song_mlp_grad)."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    wp = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+    g = np.empty_like(params)
+    loss = C.c_double()
+    _check(load_library().song_mlp_grad(out, loss_kind, params.ctypes.data, x.ctypes.data,
+                                        y.ctypes.data, wp.ctypes.data if wp is not None else None,
+                                        x.shape[0], g.ctypes.data, C.byref(loss)))
+    return g, loss.value

@@ -59,6 +59,14 @@ struct song_index {
     void* d_fp8 = nullptr;
     float* d_fp8_scale = nullptr;
     int fp8_ld = 0;
+    // learned entry / stop models
+    bool has_model = false;
+    std::vector<int32_t> hubs;
+    std::vector<float> entry_p, stop_p;  // FP32 master parameters
+    int32_t* d_hubs = nullptr;
+    __half* d_entry_w = nullptr;
+    __half* d_stop_w = nullptr;
+    int ckpt_every = 4, min_expansions = 8, model_k = 10;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
@@ -132,6 +140,9 @@ void free_index(song_index* x) {
     cudaFree(x->d_bf16);
     cudaFree(x->d_fp8);
     cudaFree(x->d_fp8_scale);
+    cudaFree(x->d_hubs);
+    cudaFree(x->d_entry_w);
+    cudaFree(x->d_stop_w);
     if (x->ev0) cudaEventDestroy(x->ev0);
     if (x->ev1) cudaEventDestroy(x->ev1);
     if (x->stream) cudaStreamDestroy(x->stream);
@@ -250,6 +261,20 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
         a->lowp_ld = prec == SONG_PREC_BF16 ? x->bf16_ld : x->fp8_ld;
         a->qdim = song::lowp_padded_dim(prec, x->dim);
         a->rerank = opts->rerank ? 1 : 0;
+    }
+    if (opts && opts->learned) {
+        if (!x->has_model) return fail(SONG_ERR_INVALID_ARG, "no learned model attached (song_index_learn)");
+        if (x->kind != SONG_KIND_L2 || cap > 1024)
+            return fail(SONG_ERR_UNSUPPORTED, "learned search: L2 indexes, queues up to 1024 slots");
+        a->lm = 2;
+        a->hubs = x->d_hubs;
+        a->n_hubs = (int)x->hubs.size();
+        a->entry_w = x->d_entry_w;
+        a->stop_w = x->d_stop_w;
+        a->ckpt_every = x->ckpt_every;
+        a->min_expansions = x->min_expansions;
+        const float t = opts->stop_threshold;
+        a->stop_thr = t <= 0.0f ? -INFINITY : (t >= 1.0f ? INFINITY : std::log(t / (1.0f - t)));
     }
     song::search_warp_smem(x->kind, a->qdim, cap, x->p.bf_words, a);
     if (cap > 4096)
@@ -553,6 +578,154 @@ song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,
                                song_query_trace* traces, song_timing* timing) {
     return host_search(index, index ? index->kind : SONG_KIND_L2, queries, nq, k, n_multiquery,
                        ef_search, ids, traces, timing, opts, dists);
+}
+
+void song_learn_params_default(song_learn_params* p) {
+    if (!p) return;
+    p->k = 10;
+    p->ef = 128;
+    p->ckpt_every = 4;
+    p->min_expansions = 8;
+    p->max_ckpt = 256;
+    p->entry_steps = 1500;
+    p->stop_steps = 3000;
+    p->batch = 4096;
+    p->lr = 2e-3f;
+    p->seed = 2020;
+}
+
+static song_status attach_model(song_index* x) {
+    cudaFree(x->d_hubs);
+    x->d_hubs = nullptr;
+    SONG_CUDA(cudaMalloc(&x->d_hubs, std::max<size_t>(1, x->hubs.size()) * 4), "hub alloc");
+    SONG_CUDA(cudaMemcpy(x->d_hubs, x->hubs.data(), x->hubs.size() * 4, cudaMemcpyHostToDevice), "hubs");
+    SONG_CUDA(song::upload_half(x->entry_p, &x->d_entry_w), "entry weights");
+    SONG_CUDA(song::upload_half(x->stop_p, &x->d_stop_w), "stop weights");
+    x->has_model = true;
+    return SONG_OK;
+}
+
+song_status song_index_learn(song_index* x, const song_learn_params* lp,
+                             const float* d_train_queries, int nq, const int32_t* d_train_nn1,
+                             song_learn_report* report) {
+    if (x == nullptr || lp == nullptr) return fail(SONG_ERR_INVALID_ARG, "index or params is NULL");
+    if (x->kind != SONG_KIND_L2) return fail(SONG_ERR_UNSUPPORTED, "learned models apply to L2 indexes");
+    if (nq < 1 || d_train_queries == nullptr || d_train_nn1 == nullptr)
+        return fail(SONG_ERR_INVALID_ARG, "training queries / nearest neighbours missing");
+    if (lp->k < 1 || lp->ef < 1 || lp->ckpt_every < 1 || lp->max_ckpt < 1 || lp->batch < 1)
+        return fail(SONG_ERR_INVALID_ARG, "bad learn parameters");
+    std::lock_guard<std::mutex> lock(x->mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != x->device) SONG_CUDA(cudaSetDevice(x->device), "cudaSetDevice");
+    const int ef = clamp_ef(lp->ef, lp->k, x->p.pq_size);
+    int32_t* d_ids = nullptr;
+    SONG_CUDA(cudaMalloc(&d_ids, (size_t)nq * lp->k * 4), "train ids alloc");
+    song::SearchArgs a;
+    song_status s = make_args(x, d_train_queries, nq, lp->k, ef, d_ids, nullptr, &a);
+    if (s != SONG_OK) {
+        cudaFree(d_ids);
+        return s;
+    }
+    a.counter = x->d_counter;
+    a.ckpt_every = lp->ckpt_every;
+    a.min_expansions = lp->min_expansions;
+    song::LearnInputs in{};
+    in.args = a;
+    in.base = x->d_base;
+    in.n = x->n;
+    in.dim = x->dim;
+    in.ld = x->ld;
+    in.nn1 = d_train_nn1;
+    in.nq = nq;
+    in.max_ckpt = lp->max_ckpt;
+    in.entry_steps = lp->entry_steps;
+    in.stop_steps = lp->stop_steps;
+    in.batch = lp->batch;
+    in.lr = lp->lr;
+    in.seed = lp->seed;
+    in.num_sms = x->num_sms;
+    in.stream = x->stream;
+    song::LearnOutputs out;
+    cudaError_t e = song::learn_models(in, &out);
+    cudaFree(d_ids);
+    if (e != cudaSuccess) return cuda_fail(e, "learn");
+    x->hubs = out.hubs;
+    x->entry_p = out.entry;
+    x->stop_p = out.stop;
+    x->ckpt_every = lp->ckpt_every;
+    x->min_expansions = lp->min_expansions;
+    x->model_k = lp->k;
+    if (song_status s2 = attach_model(x)) return s2;
+    if (report) {
+        report->n_hubs = (int)out.hubs.size();
+        report->stop_samples = out.stop_samples;
+        report->entry_loss_first = out.entry_loss_first;
+        report->entry_loss_last = out.entry_loss_last;
+        report->stop_loss_first = out.stop_loss_first;
+        report->stop_loss_last = out.stop_loss_last;
+        report->stop_pos_frac = out.stop_pos_frac;
+    }
+    return SONG_OK;
+}
+
+static const uint32_t kModelMagic = 0x534f4e47u;  // "SONG"
+
+song_status song_index_get_model(const song_index* x, float* blob, int capacity, int* length) {
+    if (x == nullptr || length == nullptr) return fail(SONG_ERR_INVALID_ARG, "index or length is NULL");
+    if (!x->has_model) return fail(SONG_ERR_INVALID_ARG, "no learned model attached");
+    std::vector<float> v;
+    auto put_u = [&](uint32_t u) { float f; std::memcpy(&f, &u, 4); v.push_back(f); };
+    put_u(kModelMagic);
+    put_u(1);
+    put_u((uint32_t)x->hubs.size());
+    put_u((uint32_t)x->ckpt_every);
+    put_u((uint32_t)x->min_expansions);
+    put_u((uint32_t)x->model_k);
+    put_u((uint32_t)x->entry_p.size());
+    put_u((uint32_t)x->stop_p.size());
+    for (int32_t h : x->hubs) put_u((uint32_t)h);
+    v.insert(v.end(), x->entry_p.begin(), x->entry_p.end());
+    v.insert(v.end(), x->stop_p.begin(), x->stop_p.end());
+    *length = (int)v.size();
+    if (blob != nullptr) {
+        if (capacity < (int)v.size()) return fail(SONG_ERR_INVALID_ARG, "blob capacity too small");
+        std::memcpy(blob, v.data(), v.size() * 4);
+    }
+    return SONG_OK;
+}
+
+song_status song_index_set_model(song_index* x, const float* blob, int length) {
+    if (x == nullptr || blob == nullptr || length < 8) return fail(SONG_ERR_INVALID_ARG, "bad model blob");
+    auto get_u = [&](int i) { uint32_t u; std::memcpy(&u, blob + i, 4); return u; };
+    if (get_u(0) != kModelMagic || get_u(1) != 1) return fail(SONG_ERR_INVALID_ARG, "not a model blob");
+    const int nh = (int)get_u(2), ne = (int)get_u(6), ns = (int)get_u(7);
+    if (nh < 1 || nh > song::kFeat || ne != song::mlp_param_count(nh) ||
+        ns != song::mlp_param_count(1) || length != 8 + nh + ne + ns)
+        return fail(SONG_ERR_INVALID_ARG, "model blob sizes do not match");
+    std::lock_guard<std::mutex> lock(x->mu);
+    x->hubs.resize(nh);
+    for (int i = 0; i < nh; ++i) {
+        x->hubs[i] = (int32_t)get_u(8 + i);
+        if (x->hubs[i] < 0 || x->hubs[i] >= x->n) return fail(SONG_ERR_INVALID_ARG, "hub id out of range");
+    }
+    x->ckpt_every = (int)get_u(3);
+    x->min_expansions = (int)get_u(4);
+    x->model_k = (int)get_u(5);
+    x->entry_p.assign(blob + 8 + nh, blob + 8 + nh + ne);
+    x->stop_p.assign(blob + 8 + nh + ne, blob + 8 + nh + ne + ns);
+    return attach_model(x);
+}
+
+song_status song_mlp_grad(int out, int loss_kind, const float* params, const float* x,
+                          const float* y, const float* sample_weight, int batch, float* grad,
+                          double* loss) {
+    if (out < 1 || out > 64 || (loss_kind == 0 && out != 1) || loss_kind < 0 || loss_kind > 1 ||
+        batch < 1 || !params || !x || !y || !grad || !loss)
+        return fail(SONG_ERR_INVALID_ARG, "bad mlp_grad arguments");
+    cudaError_t e = song::mlp_grad(params, out, loss_kind, x, y, sample_weight, batch, grad, loss);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp_grad");
+    return SONG_OK;
 }
 
 int64_t song_kernel_launch_count(void) { return song::g_launches.load(); }

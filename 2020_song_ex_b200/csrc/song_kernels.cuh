@@ -2,6 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cuda_fp16.h>
+
+#include <vector>
 
 #include "song_b200.h"
 
@@ -39,7 +42,29 @@ struct SearchArgs {
     int qdim;                // floats of the query kept in shared memory (padded dim)
     int rerank;              // 1: exact FP32 re-rank of the final results queue
     float* out_dist;         // [nq x k] distance of each output id (nullable)
+    // learned entry / stop (lm: 0 off, 1 collect traces of the full search, 2 infer)
+    int lm;
+    const int32_t* hubs;     // [n_hubs] entry hub node ids (n_hubs <= kFeat)
+    int n_hubs;
+    const __half* entry_w;   // packed entry MLP (kFeat -> kHid -> kHid -> n_hubs), nullable
+    const __half* stop_w;    // packed stop MLP (kFeat -> kHid -> kHid -> 1), nullable
+    int ckpt_every;          // expansions between stop checkpoints
+    int min_expansions;      // no learned stop before this many expansions
+    float stop_thr;          // stop when sigmoid(stop logit) >= stop_thr
+    int max_ckpt;            // checkpoints per query in the trace buffers
+    float* tr_feat;          // [nq x max_ckpt x kFeat] stop features
+    float* tr_kth;           // [nq x max_ckpt] k-th best distance at each checkpoint
+    int* tr_count;           // [nq] checkpoints written
+    float* tr_final_kth;     // [nq] k-th best distance at the end of the search
+    float* tr_entry_feat;    // [nq x kFeat] entry features (hub distances)
 };
+
+// Learned model geometry: kFeat inputs, two hidden layers of kHid (ReLU).
+constexpr int kFeat = 24;
+constexpr int kHid = 64;
+// Packed FP16 / FP32 parameter layout: W1[kHid][kFeat] b1[kHid] W2[kHid][kHid] b2[kHid]
+// W3[out][kHid] b3[out].
+constexpr int mlp_param_count(int out) { return kHid * kFeat + kHid + kHid * kHid + kHid + out * kHid + out; }
 
 // Padded element count of a compressed row (a whole number of 128-byte
 // lines per 8-lane group) and its byte stride.
@@ -81,6 +106,31 @@ cudaError_t build_graph_with_scratch(int kind, const void* d_base, int64_t n, in
                                      const song_params& p, int ratio, int bf_words,
                                      int32_t* d_adj, int num_sms, cudaStream_t st, void* scratch,
                                      size_t scratch_bytes);
+
+// Training of the learned entry / stop models (song_learn.cu).
+struct LearnInputs {
+    SearchArgs args;         // plain full-budget search over the training queries (cap = ef, k)
+    const void* base;        // FP32 rows [n x ld]
+    int64_t n;
+    int dim, ld;
+    const int32_t* nn1;      // [nq] exact nearest neighbour of each training query
+    int nq, max_ckpt, entry_steps, stop_steps, batch;
+    float lr;
+    uint64_t seed;
+    int num_sms;
+    cudaStream_t stream;
+};
+struct LearnOutputs {
+    std::vector<int32_t> hubs;
+    std::vector<float> entry, stop;  // FP32 master parameters (packed layout)
+    double entry_loss_first = 0, entry_loss_last = 0, stop_loss_first = 0, stop_loss_last = 0;
+    double stop_pos_frac = 0;
+    int64_t stop_samples = 0;
+};
+cudaError_t learn_models(const LearnInputs& in, LearnOutputs* out);
+cudaError_t upload_half(const std::vector<float>& P, __half** d);
+cudaError_t mlp_grad(const float* hP, int out, int loss_kind, const float* hX, const float* hY,
+                     const float* hW, int B, float* hG, double* loss);
 
 // Records a failure message for song_last_error() on the calling thread.
 song_status set_error(song_status status, const char* message);

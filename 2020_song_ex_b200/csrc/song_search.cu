@@ -647,11 +647,149 @@ __device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL>& re
     return cnt;
 }
 
+
+// ------------------------------------------------------------ learned model
+
+// Warp-resident MLP over warp-uniform inputs f[kFeat] with FP16 weights and
+// FP32 accumulation: relu(W1 f + b1) -> relu(W2 h + b2) -> W3 h + b3.
+// Lane l evaluates hidden units l and l + 32.  For n_out == 1 every lane
+// returns the output; otherwise lane o < n_out (<= 32) returns output o.
+__device__ __forceinline__ float mlp_warp(const __half* __restrict__ w, const float (&f)[kFeat],
+                                          int n_out, int lane) {
+    const __half* W1 = w;
+    const __half* b1 = W1 + kHid * kFeat;
+    const __half* W2 = b1 + kHid;
+    const __half* b2 = W2 + kHid * kHid;
+    const __half* W3 = b2 + kHid;
+    const __half* b3 = W3 + n_out * kHid;
+    float h0 = __half2float(b1[lane]), h1 = __half2float(b1[lane + 32]);
+    const __half2* r0 = reinterpret_cast<const __half2*>(W1 + lane * kFeat);
+    const __half2* r1 = reinterpret_cast<const __half2*>(W1 + (lane + 32) * kFeat);
+#pragma unroll
+    for (int i = 0; i < kFeat / 2; ++i) {
+        const float2 a = __half22float2(r0[i]);
+        const float2 b = __half22float2(r1[i]);
+        h0 = fmaf(a.x, f[2 * i], h0);
+        h0 = fmaf(a.y, f[2 * i + 1], h0);
+        h1 = fmaf(b.x, f[2 * i], h1);
+        h1 = fmaf(b.y, f[2 * i + 1], h1);
+    }
+    h0 = fmaxf(h0, 0.0f);
+    h1 = fmaxf(h1, 0.0f);
+    float g0 = __half2float(b2[lane]), g1 = __half2float(b2[lane + 32]);
+    const __half2* s0 = reinterpret_cast<const __half2*>(W2 + lane * kHid);
+    const __half2* s1 = reinterpret_cast<const __half2*>(W2 + (lane + 32) * kHid);
+#pragma unroll 4
+    for (int j = 0; j < 32; j += 2) {
+        const float x0 = __shfl_sync(FULL, h0, j), x1 = __shfl_sync(FULL, h0, j + 1);
+        const float y0 = __shfl_sync(FULL, h1, j), y1 = __shfl_sync(FULL, h1, j + 1);
+        const float2 a = __half22float2(s0[j >> 1]), c = __half22float2(s0[(j + 32) >> 1]);
+        const float2 b = __half22float2(s1[j >> 1]), e = __half22float2(s1[(j + 32) >> 1]);
+        g0 = fmaf(a.x, x0, fmaf(a.y, x1, fmaf(c.x, y0, fmaf(c.y, y1, g0))));
+        g1 = fmaf(b.x, x0, fmaf(b.y, x1, fmaf(e.x, y0, fmaf(e.y, y1, g1))));
+    }
+    g0 = fmaxf(g0, 0.0f);
+    g1 = fmaxf(g1, 0.0f);
+    if (n_out == 1) {
+        float z = fmaf(__half2float(W3[lane]), g0, __half2float(W3[lane + 32]) * g1);
+#pragma unroll
+        for (int w2 = 16; w2 >= 1; w2 >>= 1) z += __shfl_xor_sync(FULL, z, w2);
+        return z + __half2float(b3[0]);
+    }
+    const int o = lane < n_out ? lane : 0;
+    const __half2* t3 = reinterpret_cast<const __half2*>(W3 + o * kHid);
+    float z = __half2float(b3[o]);
+#pragma unroll 4
+    for (int j = 0; j < 32; j += 2) {
+        const float x0 = __shfl_sync(FULL, g0, j), x1 = __shfl_sync(FULL, g0, j + 1);
+        const float y0 = __shfl_sync(FULL, g1, j), y1 = __shfl_sync(FULL, g1, j + 1);
+        const float2 a = __half22float2(t3[j >> 1]), c = __half22float2(t3[(j + 32) >> 1]);
+        z = fmaf(a.x, x0, fmaf(a.y, x1, fmaf(c.x, y0, fmaf(c.y, y1, z))));
+    }
+    return z;
+}
+
+// Running statistics of a search for the learned stop.  kd: lane i < K holds
+// the i-th smallest distance computed so far (+inf if fewer), which is the
+// i-th entry of the results' top-K, since results only lose their maximum.
+struct StopState {
+    float kd, kth, best, kth_prev, entry_d;
+    int K, hops_kth, hops_best, n_new, n_res, n_front, nck;
+};
+
+__device__ __forceinline__ void stop_init(StopState& s, int k) {
+    s.kd = s.kth = s.best = s.kth_prev = s.entry_d = INFINITY;
+    s.K = k < 1 ? 1 : (k > 32 ? 32 : k);
+    s.hops_kth = s.hops_best = s.n_new = s.n_res = s.n_front = s.nck = 0;
+}
+
+// Insert the distances of the lanes in N into the sorted top-K (lane order).
+__device__ __forceinline__ void topk_insert(StopState& s, unsigned N, float d, int lane) {
+    const bool mine = (N >> lane) & 1u;
+    unsigned ins = __ballot_sync(FULL, mine && d < s.kth);
+    while (ins) {
+        const int j = __ffs(ins) - 1;
+        const float v = __shfl_sync(FULL, d, j);
+        const int p = __popc(__ballot_sync(FULL, lane < s.K && s.kd <= v));
+        const float up = __shfl_up_sync(FULL, s.kd, 1);
+        if (lane < s.K && lane > p) s.kd = up;
+        if (lane == p) s.kd = v;
+        if (v < s.best) s.hops_best = 0;
+        const float nk = __shfl_sync(FULL, s.kd, s.K - 1);
+        if (nk != s.kth) s.hops_kth = 0;
+        s.kth = nk;
+        s.best = __shfl_sync(FULL, s.kd, 0);
+        ins &= ~(1u << j);
+        ins &= __ballot_sync(FULL, mine && d < s.kth);
+    }
+}
+
+// The kFeat stop features (warp-uniform), all finite and roughly in [0, 1].
+__device__ __forceinline__ void stop_features(float (&f)[kFeat], const StopState& s, int t,
+                                              float cmin, float worst, bool res_full,
+                                              float cand_fill, float res_fill, int evals,
+                                              int window) {
+    const bool kf = s.kth < INFINITY;
+    const float kth = kf ? fmaxf(s.kth, 1e-30f) : 1.0f;
+    const float best = s.best < INFINITY ? s.best : 0.0f;
+    const float wnd = 1.0f / (float)window;
+    f[0] = log1pf((float)t) * 0.125f;
+    f[1] = kf ? fminf(cmin / kth, 4.0f) * 0.25f : 1.0f;
+    f[2] = kf ? fminf(best / kth, 1.0f) : 0.0f;
+    f[3] = (kf && s.kth_prev < INFINITY) ? fminf(s.kth / fmaxf(s.kth_prev, 1e-30f), 1.0f) : 1.0f;
+    f[4] = fminf((float)s.hops_kth, 256.0f) * (1.0f / 64.0f);
+    f[5] = fminf((float)s.hops_best, 256.0f) * (1.0f / 64.0f);
+    f[6] = (res_full && kf) ? fminf(worst / kth, 8.0f) * 0.125f : 1.0f;
+    f[7] = (float)s.n_res * wnd;
+    f[8] = (float)s.n_new * wnd;
+    f[9] = cand_fill;
+    f[10] = res_fill;
+    f[11] = kf ? fminf(logf(kth / fmaxf(best, 1e-30f)), 8.0f) * 0.125f : 1.0f;
+    f[12] = log1pf((float)s.hops_kth) * (1.0f / 6.0f);
+    f[13] = log1pf((float)s.hops_best) * (1.0f / 6.0f);
+    f[14] = res_full ? fminf(cmin / fmaxf(worst, 1e-30f), 2.0f) * 0.5f : 0.0f;
+    f[15] = (float)evals / (float)(t * 32 + 1);
+    f[16] = kf ? 1.0f : 0.0f;
+    f[17] = log1pf(kf ? s.kth : 0.0f) * (1.0f / 16.0f);
+    f[18] = log1pf(best) * (1.0f / 16.0f);
+    f[19] = log1pf(cmin < INFINITY ? cmin : 0.0f) * (1.0f / 16.0f);
+    f[20] = (float)s.n_front * wnd;
+    f[21] = (float)s.K * (1.0f / 32.0f);
+    f[22] = (kf && s.entry_d < INFINITY) ? fminf(s.entry_d / kth, 64.0f) * (1.0f / 64.0f) : 1.0f;
+    f[23] = 1.0f;
+}
+
+// Order-preserving unsigned key of a float (for redux over signed values).
+__device__ __forceinline__ unsigned fkey(float x) {
+    const unsigned b = __float_as_uint(x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
 // KIND 0 = L2 with NE query elements per lane (0: query in shared memory);
 // KIND 1 = Hamming with NE uint4 of code per row.  GPL: queue groups per lane.
 // DT: SONG_PREC_FP32 (the plain, bit-exact search) or the precision form on
 // BF16 / FP8 rows (KIND 0, query in shared memory, FP32 re-rank at the end).
-template <int KIND, int NE, int GPL, int DT>
+template <int KIND, int NE, int GPL, int DT, int LM>
 __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsigned char* ws,
                                              int lane) {
     Queue<GPL> cand, res;
@@ -727,6 +865,61 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     for (int w = lane; w < a.bf_words; w += 32) bloom[w] = 0ull;
     __syncwarp();
 
+    auto distances = [&](int nb, unsigned N) -> float {
+        float d;
+        if constexpr (DT != SONG_PREC_FP32) {
+            d = l2_lowp<DT>(a, sq, nb, N, rows, lane);
+        } else if constexpr (KIND == 0) {
+            const float* base = reinterpret_cast<const float*>(a.base);
+            if constexpr (kIntPath) {
+                if (int_exact) d = l2_int<NE>(base, a.ld, qv, nb, N, rows, lane);
+                else d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
+            } else {
+                d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
+            }
+        } else {
+            d = ham_lane<NE>(reinterpret_cast<const uint32_t*>(a.base), a.ld, qcode, nb,
+                             (N >> lane) & 1u);
+        }
+        return d;
+    };
+
+    // Learned entry: distances to the hub nodes are the entry features; the
+    // entry model's top hubs replace the p*n/N_MULTIPROBE seeds.
+    StopState ss;
+    stop_init(ss, a.k);
+    int seed_id = -1, n_seeds = a.n_multiprobe;
+    if constexpr (LM > 0) {
+        if (a.n_hubs > 0) {
+            const int hub = lane < a.n_hubs ? __ldg(a.hubs + lane) : -1;
+            const unsigned HN = __ballot_sync(FULL, hub >= 0);
+            const float hd = distances(hub, HN);
+            float dmin = hub >= 0 ? hd : INFINITY;
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, w));
+            const float rel = hub >= 0 ? hd / fmaxf(dmin, 1e-30f) : 0.0f;
+            float f[kFeat];
+#pragma unroll
+            for (int i = 0; i < kFeat; ++i) f[i] = fminf(__shfl_sync(FULL, rel, i), 64.0f) * (1.0f / 64.0f);
+            if (LM == 1 && a.tr_entry_feat != nullptr && lane < kFeat)
+                a.tr_entry_feat[(int64_t)qid * kFeat + lane] = lane < a.n_hubs ? fminf(rel, 64.0f) * (1.0f / 64.0f) : 0.0f;
+            if (a.entry_w != nullptr) {
+                const float z = mlp_warp(a.entry_w, f, a.n_hubs, lane);
+                n_seeds = a.n_multiprobe < a.n_hubs ? a.n_multiprobe : a.n_hubs;
+                if (n_seeds > 32) n_seeds = 32;
+                bool used = false;
+                for (int s2 = 0; s2 < n_seeds; ++s2) {  // hubs by decreasing score
+                    const unsigned key = (hub >= 0 && !used) ? fkey(z) : 0u;
+                    const unsigned mk = __reduce_max_sync(FULL, key);
+                    const int win = __ffs(__ballot_sync(FULL, hub >= 0 && !used && key == mk)) - 1;
+                    const int h = __shfl_sync(FULL, hub, win);
+                    if (lane == s2) seed_id = h;
+                    if (lane == win) used = true;
+                }
+            }
+        }
+    }
+
     song_query_trace tr = {};
     bool seeding = true;  // the first pass inserts the N_MULTIPROBE entry points
     for (;;) {
@@ -734,8 +927,8 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         const int32_t* arow = nullptr;
         int first = -1;  // first chunk of the adjacency row
         if (seeding) {
-            limit = a.n_multiprobe;  // seeds p*n/N_MULTIPROBE (kernalGraph.h:214-231)
-        } else {                     // expansion (kernalGraph.h:233-289)
+            limit = n_seeds;  // seeds p*n/N_MULTIPROBE (kernalGraph.h:214-231)
+        } else {              // expansion (kernalGraph.h:233-289)
             if (cand.sz == 0) break;
             unsigned mb, mi;
             root_min(cand, mb, mi);
@@ -746,12 +939,41 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             q_remove<true>(cand, (int)mi, lane);
             if (lane < limit) first = __ldg(arow + lane);
             tr.expanded_nodes += 1;
+            unsigned wb = 0xffffffffu, wi;
             if (res.sz == res.cap) {  // early stop: full and strictly worse than the worst
-                unsigned wb, wi;
                 root_max(res, wb, wi);
                 if (fbits(cmin) > wb) {
                     tr.early_stopped = 1;
                     break;
+                }
+            }
+            if constexpr (LM > 0) {  // learned-stop checkpoint
+                ss.hops_kth += 1;
+                ss.hops_best += 1;
+                const int t = tr.expanded_nodes;
+                if (t % a.ckpt_every == 0) {
+                    float f[kFeat];
+                    stop_features(f, ss, t, cmin, __uint_as_float(wb), res.sz == res.cap,
+                                  (float)cand.sz / (float)cand.cap, (float)res.sz / (float)res.cap,
+                                  tr.distance_evals, a.ckpt_every * a.block_size);
+                    if (LM == 1 && a.tr_feat != nullptr && ss.nck < a.max_ckpt) {
+                        const int64_t row = (int64_t)qid * a.max_ckpt + ss.nck;
+                        if (lane == 0) {
+#pragma unroll
+                            for (int i = 0; i < kFeat; ++i) a.tr_feat[row * kFeat + i] = f[i];
+                            a.tr_kth[row] = ss.kth;
+                        }
+                        ss.nck += 1;
+                    }
+                    if (LM == 2 && a.stop_w != nullptr && t >= a.min_expansions && ss.kth < INFINITY) {
+                        const float z = mlp_warp(a.stop_w, f, 1, lane);
+                        if (z >= a.stop_thr) {
+                            tr.early_stopped = 2;  // learned stop
+                            break;
+                        }
+                    }
+                    ss.kth_prev = ss.kth;
+                    ss.n_new = ss.n_res = ss.n_front = 0;
                 }
             }
             if (cand.sz > 0) {  // the next pop is most often today's runner-up: warm its row in L2
@@ -767,30 +989,20 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             const int j = c0 + lane;
             int nb = -1;
             if (j < limit) {
-                nb = seeding ? (int)((unsigned long long)j * (unsigned long long)a.n /
-                                     (unsigned long long)a.n_multiprobe)
-                             : (c0 == 0 ? first : __ldg(arow + j));
+                if (seeding) {
+                    nb = (LM > 0 && seed_id >= 0) ? seed_id
+                                                  : (int)((unsigned long long)j * (unsigned long long)a.n /
+                                                          (unsigned long long)a.n_multiprobe);
+                } else {
+                    nb = c0 == 0 ? first : __ldg(arow + j);
+                }
             }
             if (nb >= a.n) {  // impossible for a validated graph; never read out of range
                 atomicExch(a.err, 1);
                 nb = -1;
             }
             const unsigned N = bloom_chunk(bloom, nb, bc, lane);
-            float d;
-            if constexpr (DT != SONG_PREC_FP32) {
-                d = l2_lowp<DT>(a, sq, nb, N, rows, lane);
-            } else if constexpr (KIND == 0) {
-                const float* base = reinterpret_cast<const float*>(a.base);
-                if constexpr (kIntPath) {
-                    if (int_exact) d = l2_int<NE>(base, a.ld, qv, nb, N, rows, lane);
-                    else d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
-                } else {
-                    d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
-                }
-            } else {
-                d = ham_lane<NE>(reinterpret_cast<const uint32_t*>(a.base), a.ld, qcode, nb,
-                                 (N >> lane) & 1u);
-            }
+            const float d = distances(nb, N);
             const int c = __popc(N);
             if (seeding) {
                 tr.seed_count += c;
@@ -800,8 +1012,22 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             }
             tr.visited_nodes += c;
             tr.distance_evals += c;
-            tr.frontier_pushes += q_push<true>(cand, N, d, nb, lane);
-            tr.result_updates += q_push<false>(res, N, d, nb, lane);
+            const int pf = q_push<true>(cand, N, d, nb, lane);
+            const int pr = q_push<false>(res, N, d, nb, lane);
+            tr.frontier_pushes += pf;
+            tr.result_updates += pr;
+            if constexpr (LM > 0) {
+                topk_insert(ss, N, d, lane);
+                ss.n_new += c;
+                ss.n_res += pr;
+                ss.n_front += pf;
+                if (seeding) {
+                    float m = ((N >> lane) & 1u) ? d : INFINITY;
+#pragma unroll
+                    for (int w = 16; w >= 1; w >>= 1) m = fminf(m, __shfl_xor_sync(FULL, m, w));
+                    ss.entry_d = fminf(ss.entry_d, m);
+                }
+            }
             if (N) {
                 tr.peak_frontier = max(tr.peak_frontier, cand.sz);
                 tr.peak_results = max(tr.peak_results, res.sz);
@@ -810,6 +1036,12 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         seeding = false;
     }
 
+    if constexpr (LM == 1) {
+        if (lane == 0 && a.tr_count != nullptr) {
+            a.tr_count[qid] = ss.nck;
+            a.tr_final_kth[qid] = ss.kth;
+        }
+    }
     float* outd = a.out_dist ? a.out_dist + (int64_t)qid * a.k : nullptr;
     if (DT != SONG_PREC_FP32 && a.rerank)
         tr.result_count = rerank_finish(a, res, cand, sq, a.out + (int64_t)qid * a.k, outd, lane);
@@ -818,7 +1050,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     if (a.trace != nullptr && lane == 0) a.trace[qid] = tr;
 }
 
-template <int KIND, int NE, int GPL, int DT>
+template <int KIND, int NE, int GPL, int DT, int LM = 0>
 __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -828,7 +1060,7 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         if (lane == 0) qid = (int)atomicAdd(a.counter, 1u);
         qid = __shfl_sync(FULL, qid, 0);
         if (qid >= a.nq) break;
-        search_query<KIND, NE, GPL, DT>(a, qid, ws, lane);
+        search_query<KIND, NE, GPL, DT, LM>(a, qid, ws, lane);
     }
 }
 
@@ -887,7 +1119,19 @@ __global__ void quantize_fp8(const float* __restrict__ x, int64_t n, int dim, in
     if (lane == 0) scales[r] = scale;
 }
 
+template <int LM>
+KernelFn pick_learned(const SearchArgs& a) {
+    if (a.prec == SONG_PREC_BF16) return search_kernel<0, 0, 1, SONG_PREC_BF16, LM>;
+    if (a.prec == SONG_PREC_FP8) return search_kernel<0, 0, 1, SONG_PREC_FP8, LM>;
+    if (a.dim <= 128 && a.dim > 64) return search_kernel<0, 4, 1, 0, LM>;
+    return search_kernel<0, 0, 1, 0, LM>;
+}
+
 KernelFn pick_kernel(int kind, const SearchArgs& a) {
+    if (a.lm != 0) {  // learned entry/stop: L2, queues up to 1024 slots
+        if (kind != SONG_KIND_L2 || a.cap > 1024) return nullptr;
+        return a.lm == 1 ? pick_learned<1>(a) : pick_learned<2>(a);
+    }
     if (a.cap <= 1024) return pick_gpl<1>(kind, a);
     if (a.cap <= 2048) return pick_gpl<2>(kind, a);
     if (a.cap <= 4096) return pick_gpl<4>(kind, a);

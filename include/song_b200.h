@@ -220,6 +220,63 @@ song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,
                                int ef_search, int32_t* ids, float* dists,
                                song_query_trace* traces, song_timing* timing);
 
+/*
+ * Learned entry and stop models (no counterpart in the reference).  Two
+ * MLPs of 24 inputs and two hidden layers of 64 with FP16 weights: the entry
+ * model scores 24 hub nodes from the query's distances to them (its top
+ * N_MULTIPROBE hubs become the entry points); the stop model reads running
+ * queue statistics every ckpt_every expansions and stops the search once
+ * P(top-k final) >= song_search_opts.stop_threshold.  Both are trained on
+ * the GPU by this library's kernels from traces of the plain full-budget
+ * search; without a confident stop the search runs to its natural end.
+ */
+typedef struct song_learn_params {
+    int k;               /* top-k the stop model watches (the first min(k,32) are tracked) */
+    int ef;              /* queue size of the full-budget plain search the traces come from */
+    int ckpt_every;      /* expansions between stop checkpoints (default 4)                */
+    int min_expansions;  /* no learned stop before this many expansions (default 8)        */
+    int max_ckpt;        /* checkpoints kept per training query (default 256)              */
+    int entry_steps;     /* Adam steps of the entry model (default 1500)                   */
+    int stop_steps;      /* Adam steps of the stop model (default 3000)                    */
+    int batch;           /* minibatch (default 4096)                                       */
+    float lr;            /* Adam learning rate (default 2e-3)                              */
+    unsigned seed;
+} song_learn_params;
+
+typedef struct song_learn_report {
+    int n_hubs;
+    long long stop_samples;
+    double entry_loss_first, entry_loss_last;
+    double stop_loss_first, stop_loss_last;
+    double stop_pos_frac;  /* fraction of checkpoints whose top-k was already final */
+} song_learn_report;
+
+void song_learn_params_default(song_learn_params* p);
+
+/*
+ * Train both models for an L2 index from nq training queries (device FP32
+ * [nq x dim]) and their exact nearest neighbours (device int32 [nq]).
+ * Synchronous.  The models stay attached to the index.
+ */
+song_status song_index_learn(song_index* index, const song_learn_params* params,
+                             const float* d_train_queries, int nq, const int32_t* d_train_nn1,
+                             song_learn_report* report);
+
+/* Flat FP32 copy of the attached models (*length floats; blob may be NULL to query). */
+song_status song_index_get_model(const song_index* index, float* blob, int capacity, int* length);
+/* Attach models saved by song_index_get_model. */
+song_status song_index_set_model(song_index* index, const float* blob, int length);
+
+/*
+ * Gradient check entry point: mean loss and gradient of the packed MLP
+ * parameters (FP32, layout W1 b1 W2 b2 W3 b3) over a batch, computed by the
+ * training kernels.  loss_kind 0 = binary cross-entropy with logits (y in
+ * [0,1], out = 1), 1 = softmax cross-entropy (y = class index).  Host buffers.
+ */
+song_status song_mlp_grad(int out, int loss_kind, const float* params, const float* x,
+                          const float* y, const float* sample_weight, int batch, float* grad,
+                          double* loss);
+
 /* Number of search-kernel launches issued by this library since load. */
 int64_t song_kernel_launch_count(void);
 

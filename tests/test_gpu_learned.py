@@ -1,0 +1,74 @@
+"""The learned entry/stop models: GPU training kernels against the float64
+oracle, and what the trained models gain over the plain search."""
+import importlib
+
+import numpy as np
+import pytest
+
+from conftest import knn_graph
+from oracle import mlp
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("out,loss_kind", [(1, 0), (24, 1)])
+def test_training_gradients_match_oracle(cuda, song, out, loss_kind):
+    rng = np.random.default_rng(7 + out)
+    p = rng.normal(0, 0.2, mlp.n_params(out)).astype(np.float32)
+    x = rng.normal(0, 1, (300, mlp.FEAT)).astype(np.float32)
+    y = (rng.random(300) if loss_kind == 0 else rng.integers(0, out, 300)).astype(np.float32)
+    w = (rng.random(300) + 0.5).astype(np.float32)
+    g, loss = song.mlp_grad(p, out, loss_kind, x, y, w)
+    lo, go = mlp.loss_and_grad(p.astype(np.float64), out, loss_kind, x, y, w)
+    assert abs(loss - lo) <= 1e-5 * max(1.0, abs(lo))
+    np.testing.assert_allclose(g, go, rtol=2e-4, atol=2e-6)
+
+
+def _setup(song, ds, n=30000, nq=400, ntrain=4000):
+    torch = importlib.import_module("torch")
+    gtm = importlib.import_module("2020_song_ex_b200.groundtruth")
+    m = ds.int_mixture(n, nq, dim=128, n_comp=64, seed=61)
+    train = ds.int_mixture(n, ntrain, dim=128, n_comp=64, seed=61, query_seed=62).queries
+    adj = song.build_graph(m.base, song.Params(), batch_ratio=32)
+    g = song.KernelGraph(n, 128, m.base, song.Params(pq_size=512), adj=adj)
+    g.upload_to_gpu()
+    nn1, _ = gtm.knn(m.base, train, 1)
+    gt, _ = gtm.knn(m.base, m.queries, 10)
+    rep = song.learn(g, torch.from_numpy(train).cuda(), ntrain,
+                     torch.from_numpy(nn1[:, 0].copy()).cuda(),
+                     song.LearnParams(k=10, ef=128, entry_steps=600, stop_steps=1200))
+    return m, g, gt, rep
+
+
+def test_learned_models_gain_over_plain(cuda, song, ds):
+    m, g, gt, rep = _setup(song, ds)
+    assert rep["stop_loss_last"] < rep["stop_loss_first"]
+    assert rep["entry_loss_last"] < rep["entry_loss_first"]
+    assert 0.0 < rep["stop_pos_frac"] < 1.0 and rep["stop_samples"] > 0
+    nq = m.queries.shape[0]
+    tp, tl = song.GpuSearchTrace(), song.GpuSearchTrace()
+    ids_p, _ = song.gpu_search_ex(g, song.SearchOpts(), m.queries, nq, 10, 128, trace=tp)
+    ids_l, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=0.8),
+                                  m.queries, nq, 10, 128, trace=tl)
+    rec_p = ds.recall_at_k(ids_p, gt, 10).mean()
+    rec_l = ds.recall_at_k(ids_l, gt, 10).mean()
+    exp_p = tp.queries[:, 2].mean()
+    exp_l = tl.queries[:, 2].mean()
+    # the gain: far fewer expansions for nearly the same recall
+    assert exp_l < 0.8 * exp_p, (exp_p, exp_l)
+    assert rec_l >= rec_p - 0.03, (rec_p, rec_l)
+    assert (tl.queries[:, 11] == 2).mean() > 0.3  # most queries stopped by the model
+    # threshold 1.0 never stops early: the full-budget search with the learned entry
+    ids_f, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0),
+                                  m.queries, nq, 10, 128)
+    assert ds.recall_at_k(ids_f, gt, 10).mean() >= rec_p - 0.02
+    # saved models reproduce the same search
+    blob = song.get_model(g)
+    g2 = song.KernelGraph(g.num_nodes, 128, m.base, song.Params(pq_size=512), adj=g.adj)
+    g2.upload_to_gpu()
+    song.set_model(g2, blob)
+    ids_2, _ = song.gpu_search_ex(g2, song.SearchOpts(learned=True, stop_threshold=0.8),
+                                  m.queries, nq, 10, 128)
+    np.testing.assert_array_equal(ids_2, ids_l)
+    g.close()
+    g2.close()
