@@ -423,7 +423,7 @@ class LearnParams:
     """song_learn_params: traces come from the plain search at (k, ef)."""
     k: int = 10
     ef: int = 128
-    ckpt_every: int = 4
+    ckpt_every: int = 8
     min_expansions: int = 8
     max_ckpt: int = 256
     entry_steps: int = 1500

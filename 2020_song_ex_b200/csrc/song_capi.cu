@@ -66,7 +66,7 @@ struct song_index {
     int32_t* d_hubs = nullptr;
     __half* d_entry_w = nullptr;
     __half* d_stop_w = nullptr;
-    int ckpt_every = 4, min_expansions = 8, model_k = 10;
+    int ckpt_every = 8, min_expansions = 8, model_k = 10;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
@@ -584,7 +584,7 @@ void song_learn_params_default(song_learn_params* p) {
     if (!p) return;
     p->k = 10;
     p->ef = 128;
-    p->ckpt_every = 4;
+    p->ckpt_every = 8;
     p->min_expansions = 8;
     p->max_ckpt = 256;
     p->entry_steps = 1500;

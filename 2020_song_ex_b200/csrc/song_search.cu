@@ -60,6 +60,12 @@ __constant__ uint64_t kBloomMix[8] = {
 };
 
 __device__ __forceinline__ unsigned fbits(float x) { return __float_as_uint(x); }
+
+// Read-only loads of base rows (the read-only data path; an L1 no-allocate
+// variant measured slightly slower).
+__device__ __forceinline__ float ld_row(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float4 ld_row(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ uint4 ld_row(const uint4* p) { return __ldg(p); }
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
 // Slot queue of capacity <= 1024 * GPL.  Slots live in shared memory; the
@@ -310,7 +316,7 @@ __device__ __forceinline__ float row_partial(const float* __restrict__ row, int 
 #pragma unroll
         for (int e = 0; e < NE; ++e) {
             const int i = lane + 32 * e;
-            x[e] = i < dim ? __ldg(row + i) : 0.0f;
+            x[e] = i < dim ? ld_row(row + i) : 0.0f;
         }
 #pragma unroll
         for (int e = 0; e < NE; ++e) {
@@ -322,7 +328,7 @@ __device__ __forceinline__ float row_partial(const float* __restrict__ row, int 
         }
     } else {
         for (int i = lane; i < dim; i += 32) {
-            const float t = sq[i] - __ldg(row + i);
+            const float t = sq[i] - ld_row(row + i);
             s = fmaf(t, t, s);
         }
     }
@@ -385,9 +391,9 @@ __device__ __forceinline__ float l2_int(const float* __restrict__ base, int ld,
         const float4* pa = reinterpret_cast<const float4*>(base + (size_t)(va ? rows[ra] : 0) * ld);
         const float4* pb = reinterpret_cast<const float4*>(base + (size_t)(vb ? rows[rb] : 0) * ld);
 #pragma unroll
-        for (int e = 0; e < NV; ++e) xa[e] = va ? __ldg(pa + t + 8 * e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int e = 0; e < NV; ++e) xa[e] = va ? ld_row(pa + t + 8 * e) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int e = 0; e < NV; ++e) xb[e] = vb ? __ldg(pb + t + 8 * e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int e = 0; e < NV; ++e) xb[e] = vb ? ld_row(pb + t + 8 * e) : make_float4(0.f, 0.f, 0.f, 0.f);
         float sa = 0.0f, sb = 0.0f;
 #pragma unroll
         for (int e = 0; e < NV; ++e) {
@@ -426,7 +432,7 @@ __device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int
         const uint4* row = reinterpret_cast<const uint4*>(base + (size_t)nb * ld);
 #pragma unroll
         for (int e = 0; e < W4; ++e) {
-            const uint4 x = __ldg(row + e);
+            const uint4 x = ld_row(row + e);
             s += __popc(x.x ^ q[e].x) + __popc(x.y ^ q[e].y) + __popc(x.z ^ q[e].z) +
                  __popc(x.w ^ q[e].w);
         }
@@ -561,8 +567,8 @@ __device__ __forceinline__ float l2_lowp(const SearchArgs& a, const float* sq, i
         }
         float sa = 0.0f, sb = 0.0f;
         for (int c = t; c < nchunk; c += 8) {
-            const uint4 xa = va ? __ldg(pa + c) : make_uint4(0u, 0u, 0u, 0u);
-            const uint4 xb = vb ? __ldg(pb + c) : make_uint4(0u, 0u, 0u, 0u);
+            const uint4 xa = va ? ld_row(pa + c) : make_uint4(0u, 0u, 0u, 0u);
+            const uint4 xb = vb ? ld_row(pb + c) : make_uint4(0u, 0u, 0u, 0u);
             chunk_l2<DT>(xa, sq + c * EPC, sca, sa);
             chunk_l2<DT>(xb, sq + c * EPC, scb, sb);
         }
@@ -600,7 +606,7 @@ __device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL>& re
         const float4* row = reinterpret_cast<const float4*>(base + (size_t)id * a.ld);
         float acc = 0.0f;
         for (int c = t; c < nch; c += 8) {
-            const float4 x = v ? __ldg(row + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 x = v ? ld_row(row + c) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float4 q = *reinterpret_cast<const float4*>(sq + 4 * c);
             float u = q.x - x.x;
             acc = fmaf(u, u, acc);
@@ -745,10 +751,12 @@ __device__ __forceinline__ void topk_insert(StopState& s, unsigned N, float d, i
 }
 
 // The kFeat stop features (warp-uniform), all finite and roughly in [0, 1].
+// cnt1/cnt11/cnt125: frontier candidates closer than 1x / 1.1x / 1.25x the
+// k-th best distance (the ones that can still improve the top-k).
 __device__ __forceinline__ void stop_features(float (&f)[kFeat], const StopState& s, int t,
                                               float cmin, float worst, bool res_full,
-                                              float cand_fill, float res_fill, int evals,
-                                              int window) {
+                                              float cand_fill, float res_fill, int cnt1,
+                                              int cnt11, int cnt125, int window) {
     const bool kf = s.kth < INFINITY;
     const float kth = kf ? fmaxf(s.kth, 1e-30f) : 1.0f;
     const float best = s.best < INFINITY ? s.best : 0.0f;
@@ -768,13 +776,13 @@ __device__ __forceinline__ void stop_features(float (&f)[kFeat], const StopState
     f[12] = log1pf((float)s.hops_kth) * (1.0f / 6.0f);
     f[13] = log1pf((float)s.hops_best) * (1.0f / 6.0f);
     f[14] = res_full ? fminf(cmin / fmaxf(worst, 1e-30f), 2.0f) * 0.5f : 0.0f;
-    f[15] = (float)evals / (float)(t * 32 + 1);
+    f[15] = fminf((float)cnt1, 16.0f) * (1.0f / 16.0f);
     f[16] = kf ? 1.0f : 0.0f;
     f[17] = log1pf(kf ? s.kth : 0.0f) * (1.0f / 16.0f);
-    f[18] = log1pf(best) * (1.0f / 16.0f);
+    f[18] = fminf((float)cnt125, 64.0f) * (1.0f / 64.0f);
     f[19] = log1pf(cmin < INFINITY ? cmin : 0.0f) * (1.0f / 16.0f);
     f[20] = (float)s.n_front * wnd;
-    f[21] = (float)s.K * (1.0f / 32.0f);
+    f[21] = fminf((float)cnt11, 32.0f) * (1.0f / 32.0f);
     f[22] = (kf && s.entry_d < INFINITY) ? fminf(s.entry_d / kth, 64.0f) * (1.0f / 64.0f) : 1.0f;
     f[23] = 1.0f;
 }
@@ -951,25 +959,44 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 ss.hops_kth += 1;
                 ss.hops_best += 1;
                 const int t = tr.expanded_nodes;
+                // A checkpoint right after the k-th distance improved (hops_kth == 0 after the
+                // increment below is impossible; 1 means "improved by the last expansion")
+                // cannot be the converged state the model looks for: no evaluation then.
+                const bool want = LM == 1 || (a.stop_w != nullptr && a.stop_thr < INFINITY &&
+                                              t >= a.min_expansions && ss.kth < INFINITY &&
+                                              ss.hops_kth > 1);
                 if (t % a.ckpt_every == 0) {
-                    float f[kFeat];
-                    stop_features(f, ss, t, cmin, __uint_as_float(wb), res.sz == res.cap,
-                                  (float)cand.sz / (float)cand.cap, (float)res.sz / (float)res.cap,
-                                  tr.distance_evals, a.ckpt_every * a.block_size);
-                    if (LM == 1 && a.tr_feat != nullptr && ss.nck < a.max_ckpt) {
-                        const int64_t row = (int64_t)qid * a.max_ckpt + ss.nck;
-                        if (lane == 0) {
-#pragma unroll
-                            for (int i = 0; i < kFeat; ++i) a.tr_feat[row * kFeat + i] = f[i];
-                            a.tr_kth[row] = ss.kth;
+                    if (want) {
+                        int c1 = 0, c11 = 0, c125 = 0;
+                        const float k1 = ss.kth, k11 = ss.kth * 1.1f, k125 = ss.kth * 1.25f;
+                        for (int s2 = lane; s2 < cand.sz; s2 += 32) {
+                            const float v = cand.d[s2];
+                            c1 += v < k1;
+                            c11 += v < k11;
+                            c125 += v < k125;
                         }
-                        ss.nck += 1;
-                    }
-                    if (LM == 2 && a.stop_w != nullptr && t >= a.min_expansions && ss.kth < INFINITY) {
-                        const float z = mlp_warp(a.stop_w, f, 1, lane);
-                        if (z >= a.stop_thr) {
-                            tr.early_stopped = 2;  // learned stop
-                            break;
+                        c1 = __reduce_add_sync(FULL, (unsigned)c1);
+                        c11 = __reduce_add_sync(FULL, (unsigned)c11);
+                        c125 = __reduce_add_sync(FULL, (unsigned)c125);
+                        float f[kFeat];
+                        stop_features(f, ss, t, cmin, __uint_as_float(wb), res.sz == res.cap,
+                                      (float)cand.sz / (float)cand.cap, (float)res.sz / (float)res.cap,
+                                      c1, c11, c125, a.ckpt_every * a.block_size);
+                        if (LM == 1 && a.tr_feat != nullptr && ss.nck < a.max_ckpt) {
+                            const int64_t row = (int64_t)qid * a.max_ckpt + ss.nck;
+                            if (lane == 0) {
+#pragma unroll
+                                for (int i = 0; i < kFeat; ++i) a.tr_feat[row * kFeat + i] = f[i];
+                                a.tr_kth[row] = ss.kth;
+                            }
+                            ss.nck += 1;
+                        }
+                        if (LM == 2) {
+                            const float z = mlp_warp(a.stop_w, f, 1, lane);
+                            if (z >= a.stop_thr) {
+                                tr.early_stopped = 2;  // learned stop
+                                break;
+                            }
                         }
                     }
                     ss.kth_prev = ss.kth;

@@ -9,9 +9,16 @@ public set is not available).  The queue size ef (and the Bloom filter size)
 is the smallest point of a sweep whose recall@10 against exact GPU
 brute-force ground truth reaches 0.95.
 
+Two forms are measured.  The plain form is bit-exact with the reference
+search.  The learned form keeps BF16 rows (exact for these integer vectors)
+and uses the learned entry and stop models, trained on the GPU from traces of
+50,000 held-out queries searched by the plain form; its stop threshold is the
+fastest one whose recall@10 reaches 0.95.
+
 Outputs one JSON line (rank 0).  ``value`` is device-resident QPS (queries
-and graph already in HBM); ``e2e`` is the same through the host C-ABI call
-(gpu_search with pinned host queries, H2D + kernel + D2H in the timed region).
+and graph already in HBM) of the fastest form meeting the recall target,
+with both forms under ``forms``; ``e2e`` is the same through the host C-ABI
+call (pinned host queries, H2D + kernel + D2H in the timed region).
 
 ``--impl reference`` times the reference's own CPU search (Graph::search,
 graph.h:33-115, compiled from the reference sources into oracle/_ref) on the
@@ -46,6 +53,7 @@ BLOCK_SIZE = 32
 TARGET_RECALL = 0.95
 EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 512, 640, 768, 1024)
 BF_SWEEP = (256, 1024)
+LEARN_THRESHOLDS = (0.8, 0.85, 0.9, 0.95, 0.98)
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
 
 
@@ -136,13 +144,16 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the search kernel from the committed ncu summary."""
+def ncu_traffic(ef: int, bf_words: int):
+    """Per-launch DRAM bytes of the search kernel from the committed ncu
+    summary, when it was captured at this workload and operating point."""
     p = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
     if os.path.exists(p):
         try:
             d = json.load(open(p))
-            return d.get("bytes_per_launch_scaled"), d.get("source")
+            c = d.get("config", {})
+            if (c.get("n"), c.get("nq"), c.get("ef"), c.get("bf_words")) == (N_BASE, NQ, ef, bf_words):
+                return d.get("bytes_per_launch_scaled"), d.get("source")
         except (OSError, ValueError):
             pass
     return None, None
@@ -155,7 +166,73 @@ def bytes_per_query(trace: np.ndarray, k: int) -> np.ndarray:
     return E * DIM * 4 + X * BLOCK_SIZE * 4 + DIM * 4 + k * 4
 
 
+def _gpu_index(local: int) -> int:
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if cvd:
+        try:
+            return int(cvd.split(",")[local])
+        except (ValueError, IndexError):
+            pass
+    return local
+
+
+def timed_device(torch, dist, ws, dev, stream, steps, warmup, launch, clocks_gpu=None):
+    """Warm up, then time `steps` launches on `stream` with CUDA events
+    (barrier + synchronize on both sides, max over ranks).  Returns
+    (total_ms, per-step kernel ms list, clock summary or None)."""
+    for _ in range(warmup):
+        launch()
+    stream.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    clk = Clocks(clocks_gpu) if clocks_gpu is not None else None
+    if clk:
+        clk.__enter__()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(steps):
+        evs[i][0].record(stream)
+        launch()
+        evs[i][1].record(stream)
+    t_end.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    torch.cuda.nvtx.range_pop()
+    if ws > 1:
+        dist.barrier()
+    total = torch.tensor([t_start.elapsed_time(t_end)], device=dev)
+    if ws > 1:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    return float(total.item()), [a.elapsed_time(b) for a, b in evs], (clk.summary() if clk else None)
+
+
+def timed_host(torch, dist, ws, dev, steps, warmup, call):
+    """Time `steps` synchronous host-API calls (wall clock, max over ranks)."""
+    for _ in range(warmup):
+        call()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    h0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    dt = time.perf_counter() - h0
+    t = torch.tensor([dt], device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, ws, rank, local):
+    import ctypes as C
+
     import torch
     import torch.distributed as dist
     song = importlib.import_module("2020_song_ex_b200")
@@ -163,6 +240,7 @@ def run_ours(args, ws, rank, local):
     gtm = importlib.import_module("2020_song_ex_b200.groundtruth")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    L = song.load_library()
 
     t0 = time.time()
     base, queries = make_workload(rank)
@@ -179,7 +257,7 @@ def run_ours(args, ws, rank, local):
     d_tr = torch.empty((NQ, 12), dtype=torch.int32, device=dev)
     stream = torch.cuda.Stream(device=dev)
 
-    # operating point: fastest (ef, bf_words) with recall@10 >= 0.95
+    # ---------------- plain form: fastest (ef, bf_words) with recall@10 >= 0.95
     curve, best = [], None
     graphs = {}
     sweep = BF_SWEEP if not args.ef else (args.bf_words,)
@@ -209,9 +287,8 @@ def run_ours(args, ws, rank, local):
             g.close()
     g = graphs[best["bf_words"]]
     ef = best["ef"]
-    log(f"[rank {rank}] operating point {best}")
+    log(f"[rank {rank}] plain operating point {best}")
 
-    # traces of the operating point -> algorithmic bytes per launch
     song.search_device(g, dq, NQ, K, ef, d_ids, d_tr, stream=stream)
     stream.synchronize()
     trace = d_tr.cpu().numpy()
@@ -219,126 +296,171 @@ def run_ours(args, ws, rank, local):
     recall = float(ds.recall_at_k(ids_op, gt, K).mean())
     launch_bytes = float(bytes_per_query(trace, K).sum())
 
-    # bit-exactness at full size on a sample of queries (oracle is the checker)
     parity = None
-    if rank == 0 and not args.no_parity:
+    if rank == 0 and not args.no_parity:  # bit-exactness at full size (oracle = checker)
         import oracle
         sample = 64
         oids, otr = oracle.search_l2(base, adj, BLOCK_SIZE, queries[:sample], K, ef, pq_size=1024,
                                      bf_words=best["bf_words"])
         parity = bool((oids == ids_op[:sample]).all() and (otr == trace[:sample]).all())
 
-    # ---------------- timed region: device-resident
-    for _ in range(args.warmup):
-        song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream)
-    stream.synchronize()
-    n_launch0 = song.launch_count()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    gpu_index = local
-    cvd = os.environ.get("CUDA_VISIBLE_DEVICES")
-    if cvd:
-        try:
-            gpu_index = int(cvd.split(",")[local])
-        except (ValueError, IndexError):
-            pass
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    torch.cuda.nvtx.range_push("timed")
-    with Clocks(gpu_index) as clk:
-        t_start = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
-        t_start.record(stream)
-        for i in range(args.steps):
-            evs[i][0].record(stream)
-            song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream)
-            evs[i][1].record(stream)
-        t_end.record(stream)
-        stream.synchronize()
-        torch.cuda.synchronize()
-    torch.cuda.nvtx.range_pop()
-    if ws > 1:
-        dist.barrier()
-    launches = song.launch_count() - n_launch0
-    total_ms = t_start.elapsed_time(t_end)
-    kern_ms = [a.elapsed_time(b) for a, b in evs]
-    t = torch.tensor([total_ms], device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = ws * NQ * args.steps / (total_ms / 1e3)
-
-    # ---------------- e2e: host API, pinned host queries, H2D + kernel + D2H
+    n0 = song.launch_count()
+    plain_ms, plain_kern, clocks = timed_device(
+        torch, dist, ws, dev, stream, args.steps, args.warmup,
+        lambda: song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream),
+        clocks_gpu=_gpu_index(local))
+    plain_launches = song.launch_count() - n0
+    plain_qps = ws * NQ * args.steps / (plain_ms / 1e3)
     if args.no_e2e:
         g.close()
-        return {"value": round(value, 1), "note": "profiling case"} if rank == 0 else None
+        return {"value": round(plain_qps, 1), "note": "profiling case"} if rank == 0 else None
+
     hq = torch.from_numpy(queries).pin_memory()
     hids = torch.empty((NQ, K), dtype=torch.int32).pin_memory()
-    import ctypes as C
-    L = song.load_library()
+    hdist = torch.empty((NQ, K), dtype=torch.float32).pin_memory()
     timing = song._Timing()
 
-    def host_call():
+    def host_plain():
         st = L.song_gpu_search(g._h, C.c_void_p(hq.data_ptr()), NQ, K, NQ, ef,
                                C.c_void_p(hids.data_ptr()), None, C.byref(timing))
         if st != 0:
             raise song.SongError(st, L.song_last_error().decode())
 
-    for _ in range(args.warmup):
-        host_call()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    h0 = time.perf_counter()
-    for _ in range(args.steps):
-        host_call()
-    e2e_s = time.perf_counter() - h0
-    te = torch.tensor([e2e_s], device=dev)
-    if ws > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_s = float(te.item())
+    plain_e2e_s = timed_host(torch, dist, ws, dev, args.steps, args.warmup, host_plain)
     assert np.array_equal(hids.numpy(), ids_op), "host-API ids differ from the device path"
-    e2e = {"value": round(ws * NQ * args.steps / e2e_s, 1), "unit": "queries/s",
-           "h2d_bytes_per_step": int(queries.nbytes), "d2h_bytes_per_step": int(NQ * K * 4)}
+    plain_e2e = ws * NQ * args.steps / plain_e2e_s
+
+    # ---------------- learned form: BF16 rows + learned entry/stop
+    learned = None
+    if not args.no_learned:
+        ntrain = args.train_queries
+        train = importlib.import_module("2020_song_ex_b200.datasets").int_mixture(
+            N_BASE, ntrain, dim=DIM, n_comp=N_COMP, seed=SEED,
+            query_seed=SEED + 104729 + rank).queries
+        nn1, _ = gtm.knn(base, train, 1)
+        torch.cuda.empty_cache()
+        song.set_precision(g, song.PREC_BF16)
+        lcurve, lbest, learn_s, reps, blobs = [], None, 0.0, {}, {}
+        for lef in sorted({ef, min(1024, (ef * 3) // 2)}):
+            tl0 = time.time()
+            reps[lef] = song.learn(g, torch.from_numpy(train).to(dev), ntrain,
+                                   torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(dev),
+                                   song.LearnParams(k=K, ef=lef))
+            torch.cuda.synchronize()
+            learn_s += time.time() - tl0
+            blobs[lef] = song.get_model(g)
+            for prec in (song.PREC_FP32, song.PREC_BF16):
+                for thr in LEARN_THRESHOLDS:
+                    opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr)
+                    song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, None, stream=stream)
+                    e1.record(stream)
+                    stream.synchronize()
+                    ms = e0.elapsed_time(e1)
+                    rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
+                    trl = d_tr.cpu().numpy()
+                    pt = {"ef": lef, "precision": "bf16" if prec == song.PREC_BF16 else "fp32",
+                          "threshold": thr, "recall": round(rec, 4), "qps": round(NQ / ms * 1e3),
+                          "mean_expanded": round(float(trl[:, 2].mean()), 1),
+                          "learned_stop_rate": round(float((trl[:, 11] == 2).mean()), 3)}
+                    lcurve.append(pt)
+                    if rec >= TARGET_RECALL and (lbest is None or pt["qps"] > lbest["qps"]):
+                        lbest = pt
+        if lbest is not None:
+            lef = lbest["ef"]
+            song.set_model(g, blobs[lef])
+            rep = reps[lef]
+            lprec = song.PREC_BF16 if lbest["precision"] == "bf16" else song.PREC_FP32
+            lopts = song.SearchOpts(precision=lprec, learned=True, stop_threshold=lbest["threshold"])
+            n0 = song.launch_count()
+            lms, lkern, _ = timed_device(
+                torch, dist, ws, dev, stream, args.steps, args.warmup,
+                lambda: song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, None,
+                                              stream=stream))
+            l_launches = song.launch_count() - n0
+            ids_l = d_ids.cpu().numpy()
+            copts = lopts._c()
+
+            def host_learned():
+                st = L.song_gpu_search_ex(g._h, C.byref(copts), C.c_void_p(hq.data_ptr()), NQ, K,
+                                          NQ, lef, C.c_void_p(hids.data_ptr()),
+                                          C.c_void_p(hdist.data_ptr()), None, C.byref(timing))
+                if st != 0:
+                    raise song.SongError(st, L.song_last_error().decode())
+
+            l_e2e_s = timed_host(torch, dist, ws, dev, args.steps, args.warmup, host_learned)
+            learned = {
+                "form": f"{lbest['precision'].upper()} rows + learned entry/stop"
+                        + (" (BF16 is exact for these integer vectors)" if lbest["precision"] == "bf16" else ""),
+                "precision": lbest["precision"], "threshold": lbest["threshold"], "ef": lef,
+                "qps": round(ws * NQ * args.steps / (lms / 1e3), 1),
+                "e2e_qps": round(ws * NQ * args.steps / l_e2e_s, 1),
+                "recall_at_10": round(float(ds.recall_at_k(ids_l, gt, K).mean()), 4),
+                "ms_per_step": round(lms / args.steps, 4), "gpu_launches": int(l_launches),
+                "kernel_ms": [round(x, 3) for x in lkern],
+                "curve": lcurve, "learn_s": round(learn_s, 2), "train_queries": ntrain,
+                "learn_report": {k2: (round(v, 5) if isinstance(v, float) else v)
+                                 for k2, v in rep.items()},
+            }
+        else:
+            learned = {"curve": lcurve, "note": "no threshold reached recall 0.95",
+                       "learn_report": reps}
+        log(f"[rank {rank}] learned form {lbest}")
 
     out = None
     if rank == 0:
         peak, peak_kind = peaks()
-        avg_kern_s = statistics.mean(kern_ms) / 1e3
+        avg_kern_s = statistics.mean(plain_kern) / 1e3
         achieved = launch_bytes / avg_kern_s / 1e9
-        traffic, traffic_src = ncu_traffic()
+        traffic, traffic_src = ncu_traffic(ef, best["bf_words"])
         cpu = None if args.no_cpu_baseline else cpu_baseline(base, adj, queries, gt, ef)
         refgpu = None if args.no_ref_gpu else reference_gpu(base, adj, queries, gt, ef,
                                                             best["bf_words"], ids_op)
+        use_learned = learned is not None and "qps" in learned and learned["qps"] > plain_qps
+        value = learned["qps"] if use_learned else plain_qps
+        e2e_v = learned["e2e_qps"] if use_learned else plain_e2e
         out = {
-            "metric": "QPS at recall@10>=0.95 (plain bit-exact form)",
+            "metric": "QPS at recall@10>=0.95 (fastest form: plain bit-exact or BF16 + learned entry/stop)",
             "value": round(value, 1),
             "unit": "queries/s",
             "n_gpus": ws,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": round(total_ms / args.steps, 4),
+            "ms_per_step": round((learned["ms_per_step"] if use_learned else plain_ms / args.steps), 4),
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32",
+            "dtype": (learned["precision"] if use_learned else "f32").replace("fp32", "f32"),
             "data": "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)",
             "config": {
                 "workload": WORKLOAD, "n": N_BASE, "dim": DIM, "nq_per_gpu": NQ, "k": K,
+                "form": "learned" if use_learned else "plain",
                 "ef": ef, "bf_words": best["bf_words"], "pq_size": 1024,
                 "graph": "GPU batched-insertion NSW (ratio 32)",
                 "l2": "inputs larger than L2 (data 512 MB + adj 128 MB per GPU)",
                 "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
             },
-            "recall_at_10": round(recall, 4),
-            "operating_point": best,
+            "recall_at_10": learned["recall_at_10"] if use_learned else round(recall, 4),
+            "forms": {
+                "plain": {"qps": round(plain_qps, 1), "e2e_qps": round(plain_e2e, 1),
+                          "recall_at_10": round(recall, 4), "operating_point": best,
+                          "ms_per_step": round(plain_ms / args.steps, 4),
+                          "gpu_launches": int(plain_launches),
+                          "parity_sample_bit_exact": parity},
+                "learned": learned,
+                "learned_over_plain": (round(learned["qps"] / plain_qps, 3)
+                                       if learned and "qps" in learned else None),
+            },
             "recall_curve": curve,
-            "parity_sample_bit_exact": parity,
             "gt_fp64_spot_check": {"queries": spot[0], "ids_missed": spot[1]},
-            "e2e": e2e,
-            "gpu_launches": int(launches),
+            "e2e": {"value": round(e2e_v, 1), "unit": "queries/s",
+                    "h2d_bytes_per_step": int(queries.nbytes),
+                    "d2h_bytes_per_step": int(NQ * K * (8 if use_learned else 4))},
+            "gpu_launches": int(learned["gpu_launches"] if use_learned else plain_launches),
             "roofline": {
+                "kernel": "plain search_kernel<0,4,1,0> at the plain operating point",
                 "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                 "traffic": traffic, "traffic_source": traffic_src,
@@ -347,8 +469,8 @@ def run_ours(args, ws, rank, local):
             },
             "cpu_baseline": cpu,
             "reference_gpu_kernel": refgpu,
-            "clocks": clk.summary(),
-            "trace_means": {k: round(float(v), 2) for k, v in
+            "clocks": clocks,
+            "trace_means": {k2: round(float(v), 2) for k2, v in
                             zip(song.TRACE_FIELDS, trace.mean(axis=0))},
             "build_s": round(build_s, 2),
         }
@@ -470,6 +592,8 @@ def main(argv=None):
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned form")
+    ap.add_argument("--train-queries", type=int, default=50_000)
     ap.add_argument("--n", type=int, default=N_BASE, help="base size (profiling cases)")
     ap.add_argument("--nq", type=int, default=NQ, help="queries per GPU (profiling cases)")
     ap.add_argument("--ef", type=int, default=0, help="fixed queue size: skip the sweep")

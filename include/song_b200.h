@@ -233,7 +233,7 @@ song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,
 typedef struct song_learn_params {
     int k;               /* top-k the stop model watches (the first min(k,32) are tracked) */
     int ef;              /* queue size of the full-budget plain search the traces come from */
-    int ckpt_every;      /* expansions between stop checkpoints (default 4)                */
+    int ckpt_every;      /* expansions between stop checkpoints (default 8)                */
     int min_expansions;  /* no learned stop before this many expansions (default 8)        */
     int max_ckpt;        /* checkpoints kept per training query (default 256)              */
     int entry_steps;     /* Adam steps of the entry model (default 1500)                   */
