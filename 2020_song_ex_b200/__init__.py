@@ -100,6 +100,12 @@ class _LearnReport(C.Structure):
                 ("stop_pos_frac", C.c_double)]
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("max_k", C.c_int), ("max_ef", C.c_int), ("precision", C.c_int),
+                ("stop_threshold", C.c_float), ("ring_slots", C.c_int),
+                ("hbm_budget", C.c_longlong), ("max_ctas", C.c_int), ("idle_exit_us", C.c_int)]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -146,6 +152,17 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_index_set_model.restype = C.c_int
     L.song_mlp_grad.argtypes = [ci, ci, vp, vp, vp, vp, ci, vp, C.POINTER(C.c_double)]
     L.song_mlp_grad.restype = C.c_int
+    L.song_server_config_default.argtypes = [C.POINTER(_ServerConfig)]
+    L.song_server_config_default.restype = None
+    L.song_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
+    L.song_server_submit.argtypes = [vp, vp, ci, vp, vp, vp, C.POINTER(C.c_longlong)]
+    L.song_server_poll.argtypes = [vp, C.c_longlong, vp, vp, vp, C.POINTER(ci)]
+    L.song_server_run_poisson.argtypes = [vp, vp, ci, vp, vp, vp, C.c_double, C.c_uint, vp, vp,
+                                          C.POINTER(C.c_double)]
+    L.song_server_destroy.argtypes = [vp]
+    for name in ("song_server_create", "song_server_submit", "song_server_poll",
+                 "song_server_run_poisson", "song_server_destroy"):
+        getattr(L, name).restype = C.c_int
     for name in ("song_index_create_l2", "song_index_create_hamming", "song_index_destroy",
                  "song_index_info", "song_gpu_search", "song_gpu_search_hamming",
                  "song_search_device"):
@@ -480,3 +497,90 @@ def mlp_grad(params: np.ndarray, out: int, loss_kind: int, x, y, w=None):
                                         y.ctypes.data, wp.ctypes.data if wp is not None else None,
                                         x.shape[0], g.ctypes.data, C.byref(loss)))
     return g, loss.value
+
+
+REQ_LEARNED = 1
+
+
+@dataclass
+class ServerConfig:
+    """song_server_config (see include/song_b200.h)."""
+    max_k: int = 100
+    max_ef: int = 256
+    precision: int = PREC_FP32
+    stop_threshold: float = 0.85
+    ring_slots: int = 4096
+    hbm_budget: int = 0
+    max_ctas: int = 0
+    idle_exit_us: int = 200000
+
+    def _c(self) -> _ServerConfig:
+        return _ServerConfig(self.max_k, self.max_ef, self.precision, float(self.stop_threshold),
+                             self.ring_slots, int(self.hbm_budget), self.max_ctas,
+                             self.idle_exit_us)
+
+
+class Server:
+    """Serving loop with continuous batching over an uploaded L2 index."""
+
+    def __init__(self, g: KernelGraph, config: Optional[ServerConfig] = None):
+        self.config = config or ServerConfig()
+        self.g = g
+        self._h = C.c_void_p()
+        _check(load_library().song_server_create(g._h, C.byref(self.config._c()),
+                                                 C.byref(self._h)))
+
+    def submit(self, queries, ks, efs, flags=None) -> int:
+        q = np.ascontiguousarray(np.asarray(queries, dtype=np.float32).reshape(len(ks), -1))
+        ks = np.ascontiguousarray(ks, dtype=np.int32)
+        efs = np.ascontiguousarray(efs, dtype=np.int32)
+        fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.int32)
+        t = C.c_longlong()
+        _check(load_library().song_server_submit(self._h, q.ctypes.data, len(ks), ks.ctypes.data,
+                                                 efs.ctypes.data,
+                                                 fl.ctypes.data if fl is not None else None,
+                                                 C.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int, k: int):
+        """(done, ids[:k], dists[:k], QueryTrace row) of a ticket."""
+        ids = np.empty(self.config.max_k, dtype=np.int32)
+        d = np.empty(self.config.max_k, dtype=np.float32)
+        tr = np.zeros(12, dtype=np.int32)
+        done = C.c_int()
+        _check(load_library().song_server_poll(self._h, ticket, ids.ctypes.data, d.ctypes.data,
+                                               tr.ctypes.data, C.byref(done)))
+        return bool(done.value), ids[:k], d[:k], tr
+
+    def run_poisson(self, queries, ks, efs, flags, rate_qps: float, seed: int = 0):
+        """Native Poisson-arrival driver: (latency_ms [nq], ids [nq, max_k], wall_s)."""
+        q = np.ascontiguousarray(np.asarray(queries, dtype=np.float32))
+        nq = q.shape[0]
+        ks = np.ascontiguousarray(ks, dtype=np.int32)
+        efs = np.ascontiguousarray(efs, dtype=np.int32)
+        fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.int32)
+        lat = np.empty(nq, dtype=np.float64)
+        ids = np.empty((nq, self.config.max_k), dtype=np.int32)
+        wall = C.c_double()
+        _check(load_library().song_server_run_poisson(
+            self._h, q.ctypes.data, nq, ks.ctypes.data, efs.ctypes.data,
+            fl.ctypes.data if fl is not None else None, float(rate_qps), int(seed),
+            lat.ctypes.data, ids.ctypes.data, C.byref(wall)))
+        return lat, ids, wall.value
+
+    def close(self) -> None:
+        if self._h:
+            load_library().song_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -390,6 +390,30 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
 namespace song {
 song_status set_error(song_status status, const char* message) { return fail(status, message); }
 
+// Index-wide search arguments for a server whose slots take requests up to
+// (max_k, max_cap); per-request fields are filled by the serving kernel.
+song_status server_args(song_index* x, const song_search_opts* opts, int max_k, int max_cap,
+                        SearchArgs* a, int* num_sms, int* device) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (x->kind != SONG_KIND_L2) return fail(SONG_ERR_UNSUPPORTED, "the server serves L2 indexes");
+    song_status st = make_args(x, nullptr, 1, max_k, max_cap, nullptr, nullptr, a, opts, nullptr);
+    if (st != SONG_OK) return st;
+    a->lm = 2;
+    a->hubs = x->d_hubs;
+    a->n_hubs = x->has_model ? (int)x->hubs.size() : 0;
+    a->entry_w = x->has_model ? x->d_entry_w : nullptr;
+    a->stop_w = x->has_model ? x->d_stop_w : nullptr;
+    a->ckpt_every = x->ckpt_every;
+    a->min_expansions = x->min_expansions;
+    *num_sms = x->num_sms;
+    *device = x->device;
+    return SONG_OK;
+}
+
+int index_pq_size(const song_index* x) { return x ? x->p.pq_size : 0; }
+int index_dim(const song_index* x) { return x ? x->dim : 0; }
+bool index_has_model(const song_index* x) { return x && x->has_model; }
+
 BaseRange scan_base_range(const float* rows, int64_t n, int dim) {
     BaseRange r;
     const int64_t total = n * (int64_t)dim;

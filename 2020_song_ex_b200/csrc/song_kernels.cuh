@@ -107,6 +107,25 @@ cudaError_t build_graph_with_scratch(int kind, const void* d_base, int64_t n, in
                                      int32_t* d_adj, int num_sms, cudaStream_t st, void* scratch,
                                      size_t scratch_bytes);
 
+// Serving ring (song_serve.cu): slot = 32-byte header {long long ticket; int k;
+// int cap; int flags; ...} then the query (dim floats).
+constexpr int kServeHeader = 32;
+constexpr int kServeLearned = 1;  // request flag: learned entry/stop
+struct ServeArgs {
+    SearchArgs base;            // index-wide arguments (per-warp layout sized for max_cap)
+    const unsigned char* ring;  // device [slots x slot_bytes]
+    int slot_bytes, slots, max_k;
+    long long* head;            // device: next ticket to claim
+    const volatile long long* tail;  // device: tickets published (written by host copies)
+    const volatile int* stop;   // mapped host: shutdown flag
+    int32_t* res_ids;           // mapped host [slots x max_k]
+    float* res_dist;            // mapped host [slots x max_k]
+    song_query_trace* res_trace;  // mapped host [slots]
+    long long* res_done;        // mapped host [slots]: ticket completed in the slot
+    int max_idle_polls, sleep_ns;
+};
+cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStream_t st, int* warps_out);
+
 // Training of the learned entry / stop models (song_learn.cu).
 struct LearnInputs {
     SearchArgs args;         // plain full-budget search over the training queries (cap = ef, k)
@@ -131,6 +150,13 @@ cudaError_t learn_models(const LearnInputs& in, LearnOutputs* out);
 cudaError_t upload_half(const std::vector<float>& P, __half** d);
 cudaError_t mlp_grad(const float* hP, int out, int loss_kind, const float* hX, const float* hY,
                      const float* hW, int B, float* hG, double* loss);
+
+// Index accessors used by the server (song_capi.cu).
+song_status server_args(song_index* x, const song_search_opts* opts, int max_k, int max_cap,
+                        SearchArgs* a, int* num_sms, int* device);
+int index_pq_size(const song_index* x);
+int index_dim(const song_index* x);
+bool index_has_model(const song_index* x);
 
 // Records a failure message for song_last_error() on the calling thread.
 song_status set_error(song_status status, const char* message);

@@ -828,7 +828,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 #pragma unroll
             for (int e = 0; e < NE; ++e) {
                 const int i = lane + 32 * e;
-                qreg[e] = i < a.dim ? qg[i] : 0.0f;
+                qreg[e] = i < a.dim ? __ldcg(qg + i) : 0.0f;
                 if (i < a.dim) {
                     lo = fminf(lo, qreg[e]);
                     hi = fmaxf(hi, qreg[e]);
@@ -851,14 +851,15 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 #pragma unroll
                     for (int e = 0; e < NE; ++e) {
                         const int f = (lane & 7) + 8 * e;
-                        qv[e] = aligned ? q4[f]
-                                        : make_float4(qg[4 * f], qg[4 * f + 1], qg[4 * f + 2], qg[4 * f + 3]);
+                        qv[e] = aligned ? __ldcg(q4 + f)
+                                        : make_float4(__ldcg(qg + 4 * f), __ldcg(qg + 4 * f + 1),
+                                                      __ldcg(qg + 4 * f + 2), __ldcg(qg + 4 * f + 3));
                     }
                 }
             }
         } else {
             qreg[0] = 0.0f;
-            for (int i = lane; i < a.qdim; i += 32) sq[i] = i < a.dim ? qg[i] : 0.0f;
+            for (int i = lane; i < a.qdim; i += 32) sq[i] = i < a.dim ? __ldcg(qg + i) : 0.0f;
         }
     } else {
         const uint32_t* qg = reinterpret_cast<const uint32_t*>(a.queries) + (int64_t)qid * a.qld;
@@ -866,7 +867,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         for (int e = 0; e < NE; ++e) {
             uint32_t w[4];
 #pragma unroll
-            for (int t = 0; t < 4; ++t) w[t] = (4 * e + t) < a.dim ? qg[4 * e + t] : 0u;
+            for (int t = 0; t < 4; ++t) w[t] = (4 * e + t) < a.dim ? __ldcg(qg + 4 * e + t) : 0u;
             qcode[e] = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
@@ -1077,6 +1078,8 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     if (a.trace != nullptr && lane == 0) a.trace[qid] = tr;
 }
 
+#include "song_serve_kernel.inc"
+
 template <int KIND, int NE, int GPL, int DT, int LM = 0>
 __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1209,6 +1212,37 @@ int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a) {
     a->bl_off = round_up(a->ri_off + capr * 4, 16);
     a->warp_smem = round_up(a->bl_off + bf_words * 8, 16);
     return a->warp_smem;
+}
+
+cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStream_t st,
+                         int* warps_out) {
+    using ServeFn = void (*)(const ServeArgs);
+    ServeFn fn;
+    const SearchArgs& a = s.base;
+    if (a.prec == SONG_PREC_BF16) fn = serve_kernel<0, SONG_PREC_BF16>;
+    else if (a.prec == SONG_PREC_FP8) fn = serve_kernel<0, SONG_PREC_FP8>;
+    else if (a.dim <= 128 && a.dim > 64) fn = serve_kernel<4, 0>;
+    else fn = serve_kernel<0, 0>;
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    int warps = 8;
+    while (warps > 1 && (size_t)warps * a.warp_smem > (size_t)optin / 4) warps >>= 1;
+    const size_t smem = (size_t)warps * a.warp_smem;
+    if (smem > (size_t)optin) return cudaErrorInvalidConfiguration;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, warps * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int grid = per_sm * num_sms;
+    if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+    fn<<<grid, warps * 32, smem, st>>>(s);
+    if (warps_out) *warps_out = grid * warps;
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_search(int kind, const SearchArgs& a, int num_sms, cudaStream_t stream) {

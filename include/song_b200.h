@@ -277,6 +277,53 @@ song_status song_mlp_grad(int out, int loss_kind, const float* params, const flo
                           const float* y, const float* sample_weight, int batch, float* grad,
                           double* loss);
 
+/*
+ * Serving loop with continuous batching (no counterpart in the reference,
+ * whose gpu_search is a synchronous batch call).  A persistent kernel keeps
+ * one request per warp; requests published while others run are claimed as
+ * soon as a warp (shared-memory slot) frees up, so their work overlaps on
+ * the device.  Requests wait in a device-resident ring sized by hbm_budget;
+ * results land in pinned host memory.  Each request carries its own k (<=
+ * max_k) and queue size (clamped like gpu_search to min(max_ef, pq_size)).
+ */
+typedef struct song_server song_server;
+
+#define SONG_REQ_LEARNED 1   /* request flag: learned entry/stop (full search if not confident) */
+
+typedef struct song_server_config {
+    int max_k;             /* largest k of a request (default 100)                          */
+    int max_ef;            /* largest queue size of a request; sizes each slot (default 256) */
+    int precision;         /* SONG_PREC_* used by every request                             */
+    float stop_threshold;  /* learned stop threshold for requests flagged SONG_REQ_LEARNED  */
+    int ring_slots;        /* requests queued or running at once (default 4096)             */
+    long long hbm_budget;  /* device bytes the request ring may take (0 = no cap)           */
+    int max_ctas;          /* persistent CTAs (0 = as many as fit)                          */
+    int idle_exit_us;      /* idle warps exit after about this long (default 200000)        */
+} song_server_config;
+
+void song_server_config_default(song_server_config* c);
+song_status song_server_create(song_index* index, const song_server_config* config,
+                               song_server** out);
+/* Queue n requests (host queries [n x dim], per-request k, ef, flags).  All
+ * or nothing: SONG_ERR_BUDGET if the ring has no room.  *first_ticket gets
+ * the ticket of the first request; the rest follow consecutively.  Poll a
+ * ticket's results before ring_slots later requests reuse its slot. */
+song_status song_server_submit(song_server* s, const float* queries, int n, const int* ks,
+                               const int* efs, const int* flags, long long* first_ticket);
+/* *done = 1 and ids/dists/trace (host, nullable) filled when the ticket finished. */
+song_status song_server_poll(song_server* s, long long ticket, int32_t* ids, float* dists,
+                             song_query_trace* trace, int* done);
+/* Native Poisson driver: nq requests arriving at rate_qps (exponential gaps,
+ * seeded), submitted as they arrive, completions observed by polling.
+ * latency_ms[i] = completion - arrival of request i.  ids_out (nullable)
+ * [nq x max_k]; *wall_s = first arrival to last completion. */
+song_status song_server_run_poisson(song_server* s, const float* queries, int nq, const int* ks,
+                                    const int* efs, const int* flags, double rate_qps,
+                                    unsigned seed, double* latency_ms, int32_t* ids_out,
+                                    double* wall_s);
+/* Stops the kernel (each warp exits at its next poll) and frees the server. */
+song_status song_server_destroy(song_server* s);
+
 /* Number of search-kernel launches issued by this library since load. */
 int64_t song_kernel_launch_count(void);
 
