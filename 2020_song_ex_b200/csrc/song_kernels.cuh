@@ -117,12 +117,14 @@ struct ServeArgs {
     int slot_bytes, slots, max_k;
     long long* head;            // device: next ticket to claim
     const volatile long long* tail;  // device: tickets published (written by host copies)
-    const volatile int* stop;   // mapped host: shutdown flag
+    const volatile long long* stop;  // device: non-zero = shut down (set by a host copy)
     int32_t* res_ids;           // mapped host [slots x max_k]
     float* res_dist;            // mapped host [slots x max_k]
     song_query_trace* res_trace;  // mapped host [slots]
     long long* res_done;        // mapped host [slots]: ticket completed in the slot
-    int max_idle_polls, sleep_ns;
+    long long* last_claim;      // device: %globaltimer (ns) of the latest claim
+    long long idle_ns;          // a warp leaves once no request was claimed for this long
+    int max_idle_polls, sleep_ns;  // hard bound on consecutive empty polls; poll backoff cap
 };
 cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStream_t st, int* warps_out);
 

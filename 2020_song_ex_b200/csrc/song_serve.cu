@@ -32,10 +32,10 @@ struct song_server {
     int dim = 0, num_sms = 0, device = 0, cap_limit = 0, warps = 0;
     int slots = 0, slot_bytes = 0;
     unsigned char* d_ring = nullptr;
-    long long* d_ctrl = nullptr;       // [0] head, [1] tail
+    long long* d_ctrl = nullptr;       // [0] head, [1] tail, [2] stop, [3] last claim time
     unsigned char* h_stage = nullptr;  // pinned staging of ring slots
     long long* h_tailbuf = nullptr;    // pinned tail values, one per slot
-    int* h_stop = nullptr;             // mapped
+    long long* h_stop = nullptr;       // pinned source of the stop word
     int32_t* h_ids = nullptr;          // mapped [slots x max_k]
     float* h_dist = nullptr;           // mapped [slots x max_k]
     song_query_trace* h_trace = nullptr;  // mapped [slots]
@@ -80,7 +80,11 @@ song_status ensure_running(song_server* v) {
 
 void free_server(song_server* v) {
     if (!v) return;
-    if (v->h_stop) *reinterpret_cast<volatile int*>(v->h_stop) = 1;
+    if (v->h_stop && v->d_ctrl && v->cst) {  // every warp exits at its next poll
+        *v->h_stop = 1;
+        cudaMemcpyAsync(v->d_ctrl + 2, v->h_stop, 8, cudaMemcpyHostToDevice, v->cst);
+        cudaStreamSynchronize(v->cst);
+    }
     if (v->kst) cudaStreamSynchronize(v->kst);
     if (v->cst) cudaStreamSynchronize(v->cst);
     cudaFree(v->d_ring);
@@ -190,7 +194,7 @@ song_status song_server_create(song_index* index, const song_server_config* cfg,
     if (e == cudaSuccess) e = cudaMemset(v->d_ctrl, 0, 64);
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_stage, (size_t)v->slots * v->slot_bytes, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_tailbuf, (size_t)v->slots * 8, cudaHostAllocDefault);
-    if (e == cudaSuccess) e = cudaHostAlloc(&v->h_stop, 64, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostAlloc(&v->h_stop, 64, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_ids, nk * 4, cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_dist, nk * 4, cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_trace, (size_t)v->slots * sizeof(song_query_trace), cudaHostAllocMapped);
@@ -213,13 +217,16 @@ song_status song_server_create(song_index* index, const song_server_config* cfg,
     s.max_k = cfg->max_k;
     s.head = v->d_ctrl;
     s.tail = v->d_ctrl + 1;
-    s.stop = v->h_stop;
+    s.stop = v->d_ctrl + 2;
     s.res_ids = v->h_ids;
     s.res_dist = v->h_dist;
     s.res_trace = v->h_trace;
     s.res_done = v->h_done;
+    s.last_claim = v->d_ctrl + 3;
+    s.idle_ns = (long long)cfg->idle_exit_us * 1000;
     s.sleep_ns = 2000;
-    s.max_idle_polls = std::max(1, cfg->idle_exit_us / 2);
+    // hard bound: 64x the polls the idle time allows at the longest backoff
+    s.max_idle_polls = (int)std::min<long long>(INT32_MAX, (long long)cfg->idle_exit_us * 32);
     *out = v;
     return SONG_OK;
 }
@@ -289,6 +296,10 @@ song_status song_server_run_poisson(song_server* v, const float* queries, int nq
     const auto t0 = clk::now();
     double last = 0.0;
     long long spins = 0;
+    // Arrivals are published in small batches: once 16 are pending or the
+    // oldest has waited 10 us (each publish is two stream-ordered copies).
+    constexpr int kBatch = 16;
+    constexpr double kWindow = 10e-6;
     while (ndone < nq) {
         const double now = std::chrono::duration<double>(clk::now() - t0).count();
         int m = 0;
@@ -298,7 +309,8 @@ song_status song_server_run_poisson(song_server* v, const float* queries, int nq
             if (tk - first >= v->slots && !seen[tk - first - v->slots]) break;
             ++m;
         }
-        if (m > 0) {
+        const bool last_batch = sub + m == nq;
+        if (m > 0 && (m >= kBatch || last_batch || now - arrive[sub] >= kWindow)) {
             song_status st = publish(v, first + sub, queries + (size_t)sub * v->dim, m,
                                      ks ? ks + sub : nullptr, efs ? efs + sub : nullptr,
                                      flags ? flags + sub : nullptr);

@@ -409,6 +409,11 @@ def run_ours(args, ws, rank, local):
                        "learn_report": reps}
         log(f"[rank {rank}] learned form {lbest}")
 
+    # ---------------- serving: Poisson arrivals, mixed k / queue size, p50/p99 latency
+    serving = None
+    if not args.no_serving:
+        serving = run_serving(song, ds, gtm, torch, g, base, queries, dev, args, rank)
+
     out = None
     if rank == 0:
         peak, peak_kind = peaks()
@@ -467,6 +472,7 @@ def run_ours(args, ws, rank, local):
                 "algorithmic_bytes_per_launch": round(launch_bytes),
                 "kernel_ms_avg": round(avg_kern_s * 1e3, 4),
             },
+            "serving": serving,
             "cpu_baseline": cpu,
             "reference_gpu_kernel": refgpu,
             "clocks": clocks,
@@ -476,6 +482,53 @@ def run_ours(args, ws, rank, local):
         }
     g.close()
     return out
+
+
+SERVE_KS = (1, 10, 100)
+SERVE_EFS = (32, 64, 128, 256)
+SERVE_RATES = (5_000, 20_000, 50_000, 100_000, 200_000)
+
+
+def run_serving(song, ds, gtm, torch, g, base, queries, dev, args, rank):
+    """Continuous-batching server over the same index: Poisson arrivals at
+    several rates, k ~ U{1,10,100}, queue ~ U{32,...,256}; every request uses
+    the learned entry/stop (trained here at queue 256, k 10) and falls back to
+    the full search when not confident.  Per rate: achieved QPS, p50/p99
+    latency (arrival to completion seen by the host), recall@k per k."""
+    ntrain = min(args.train_queries, 20_000)
+    train = ds.int_mixture(N_BASE, ntrain, dim=DIM, n_comp=N_COMP, seed=SEED,
+                           query_seed=SEED + 7 * 104729 + rank).queries
+    nn1, _ = gtm.knn(base, train, 1)
+    gt100, _ = gtm.knn(base, queries, 100)
+    torch.cuda.empty_cache()
+    song.learn(g, torch.from_numpy(train).to(dev), ntrain,
+               torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(dev),
+               song.LearnParams(k=10, ef=max(SERVE_EFS)))
+    rng = np.random.default_rng(SEED + rank)
+    out = []
+    cfg = song.ServerConfig(max_k=max(SERVE_KS), max_ef=max(SERVE_EFS), stop_threshold=0.85)
+    with song.Server(g, cfg) as srv:
+        for rate in SERVE_RATES:
+            nreq = int(min(len(queries), max(2000, rate * args.serve_seconds)))
+            idx = rng.integers(0, len(queries), nreq)
+            ks = rng.choice(SERVE_KS, nreq).astype(np.int32)
+            efs = rng.choice(SERVE_EFS, nreq).astype(np.int32)
+            flags = np.full(nreq, song.REQ_LEARNED, np.int32)
+            lat, ids, wall = srv.run_poisson(queries[idx], ks, efs, flags, float(rate),
+                                             seed=int(rate))
+            rec = {}
+            for k in SERVE_KS:
+                sel = ks == k
+                if sel.any():
+                    rec[f"recall@{k}"] = round(float(ds.recall_at_k(ids[sel, :k], gt100[idx[sel], :k], k).mean()), 4)
+            out.append({"offered_qps": rate, "requests": nreq,
+                        "achieved_qps": round(nreq / wall, 1) if wall > 0 else None,
+                        "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                        "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                        "mean_ms": round(float(lat.mean()), 3), **rec})
+            log(f"[rank {rank}] serving {out[-1]}")
+    return {"form": "FP32 + learned entry/stop (full search when not confident)",
+            "k_choices": list(SERVE_KS), "queue_choices": list(SERVE_EFS), "points": out}
 
 
 def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
@@ -594,6 +647,8 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned form")
     ap.add_argument("--train-queries", type=int, default=50_000)
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--n", type=int, default=N_BASE, help="base size (profiling cases)")
     ap.add_argument("--nq", type=int, default=NQ, help="queries per GPU (profiling cases)")
     ap.add_argument("--ef", type=int, default=0, help="fixed queue size: skip the sweep")
