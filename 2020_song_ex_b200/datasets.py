@@ -174,6 +174,43 @@ def recall_at_k(ids: np.ndarray, gt: np.ndarray, k: int) -> np.ndarray:
     return hits / float(k)
 
 
+GRAPH_MAGIC = 0x3148505247474E53  # the bytes "SNGGRPH1" read as a little-endian u64
+
+
+def save_graph(path: str, adj: np.ndarray) -> None:
+    """Write an adjacency in the ``song_graph`` v1 format: u64 magic, u32
+    version (1), u32 block_size, u64 n, then int32 [n x block_size] exactly as
+    the reference's in-memory ``adj`` (graph.h:14-15; -1 = empty slot).  The
+    reference itself never serialises its graph (it rebuilds it every run)."""
+    adj = np.ascontiguousarray(adj, dtype=np.int32)
+    n, bs = adj.shape
+    with open(path, "wb") as f:
+        np.array([GRAPH_MAGIC], dtype=np.uint64).tofile(f)
+        np.array([1, bs], dtype=np.uint32).tofile(f)
+        np.array([n], dtype=np.uint64).tofile(f)
+        adj.tofile(f)
+
+
+def load_graph(path: str) -> np.ndarray:
+    """Read a ``song_graph`` v1 file; raises ValueError on a malformed file."""
+    with open(path, "rb") as f:
+        head = f.read(24)
+        if len(head) != 24:
+            raise ValueError(f"{path}: truncated graph header")
+        magic = int(np.frombuffer(head[:8], dtype=np.uint64)[0])
+        ver, bs = (int(x) for x in np.frombuffer(head[8:16], dtype=np.uint32))
+        n = int(np.frombuffer(head[16:24], dtype=np.uint64)[0])
+        if magic != GRAPH_MAGIC or ver != 1 or bs < 1:
+            raise ValueError(f"{path}: not a song_graph v1 file")
+        adj = np.fromfile(f, dtype=np.int32)
+    if adj.size != n * bs:
+        raise ValueError(f"{path}: expected {n * bs} entries, found {adj.size}")
+    adj = adj.reshape(n, bs)
+    if adj.size and (adj.min() < -1 or adj.max() >= n):
+        raise ValueError(f"{path}: neighbour id out of range")
+    return adj
+
+
 def cache_dir() -> str:
     d = os.environ.get("SONG_CACHE_DIR") or os.path.join(
         os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "_cache")

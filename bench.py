@@ -126,8 +126,9 @@ def make_workload(rank: int):
     """Same base on every rank (replicas); rank r > 0 draws its own queries
     from the same mixture."""
     ds = importlib.import_module("2020_song_ex_b200.datasets")
+    rep = importlib.import_module("2020_song_ex_b200.replicas")
     m = ds.int_mixture(N_BASE, NQ, dim=DIM, n_comp=N_COMP, seed=SEED,
-                       query_seed=None if rank == 0 else SEED + 7919 * rank)
+                       query_seed=rep.query_seed(SEED, rank))
     return m.base, m.queries
 
 
@@ -144,16 +145,19 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(ef: int, bf_words: int):
+def ncu_traffic(ef: int, bf_words: int, form: str = "plain"):
     """Per-launch DRAM bytes of the search kernel from the committed ncu
-    summary, when it was captured at this workload and operating point."""
+    summary, when it was captured at this workload, form and operating point."""
     p = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
     if os.path.exists(p):
         try:
             d = json.load(open(p))
-            c = d.get("config", {})
-            if (c.get("n"), c.get("nq"), c.get("ef"), c.get("bf_words")) == (N_BASE, NQ, ef, bf_words):
-                return d.get("bytes_per_launch_scaled"), d.get("source")
+            entries = d if isinstance(d, list) else [d]
+            for e in entries:
+                c = e.get("config", {})
+                if (c.get("n"), c.get("nq"), c.get("ef"), c.get("bf_words"), c.get("form", "plain")) == \
+                        (N_BASE, NQ, ef, bf_words, form):
+                    return e.get("bytes_per_launch_scaled"), e.get("source")
         except (OSError, ValueError):
             pass
     return None, None
@@ -207,10 +211,9 @@ def timed_device(torch, dist, ws, dev, stream, steps, warmup, launch, clocks_gpu
     torch.cuda.nvtx.range_pop()
     if ws > 1:
         dist.barrier()
-    total = torch.tensor([t_start.elapsed_time(t_end)], device=dev)
-    if ws > 1:
-        dist.all_reduce(total, op=dist.ReduceOp.MAX)
-    return float(total.item()), [a.elapsed_time(b) for a, b in evs], (clk.summary() if clk else None)
+    rep = importlib.import_module("2020_song_ex_b200.replicas")
+    total = rep.max_over_ranks(t_start.elapsed_time(t_end), device=dev)
+    return total, [a.elapsed_time(b) for a, b in evs], (clk.summary() if clk else None)
 
 
 def timed_host(torch, dist, ws, dev, steps, warmup, call):
@@ -224,10 +227,8 @@ def timed_host(torch, dist, ws, dev, steps, warmup, call):
     for _ in range(steps):
         call()
     dt = time.perf_counter() - h0
-    t = torch.tensor([dt], device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    rep = importlib.import_module("2020_song_ex_b200.replicas")
+    return rep.max_over_ranks(dt, device=dev)
 
 
 def run_ours(args, ws, rank, local):
@@ -381,6 +382,9 @@ def run_ours(args, ws, rank, local):
                                               stream=stream))
             l_launches = song.launch_count() - n0
             ids_l = d_ids.cpu().numpy()
+            song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
+            stream.synchronize()
+            l_bytes = float(bytes_per_query(d_tr.cpu().numpy(), K).sum())
             copts = lopts._c()
 
             def host_learned():
@@ -399,6 +403,8 @@ def run_ours(args, ws, rank, local):
                 "e2e_qps": round(ws * NQ * args.steps / l_e2e_s, 1),
                 "recall_at_10": round(float(ds.recall_at_k(ids_l, gt, K).mean()), 4),
                 "ms_per_step": round(lms / args.steps, 4), "gpu_launches": int(l_launches),
+                "algorithmic_bytes_per_launch": round(l_bytes),
+                "kernel_ms_avg": round(statistics.mean(lkern), 4),
                 "kernel_ms": [round(x, 3) for x in lkern],
                 "curve": lcurve, "learn_s": round(learn_s, 2), "train_queries": ntrain,
                 "learn_report": {k2: (round(v, 5) if isinstance(v, float) else v)
@@ -420,10 +426,30 @@ def run_ours(args, ws, rank, local):
         avg_kern_s = statistics.mean(plain_kern) / 1e3
         achieved = launch_bytes / avg_kern_s / 1e9
         traffic, traffic_src = ncu_traffic(ef, best["bf_words"])
+        roof_plain = {
+            "kernel": "plain search_kernel<0,4,1,0,0> (bit-exact form)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": traffic, "traffic_source": traffic_src,
+            "algorithmic_bytes_per_launch": round(launch_bytes),
+            "kernel_ms_avg": round(avg_kern_s * 1e3, 4),
+        }
         cpu = None if args.no_cpu_baseline else cpu_baseline(base, adj, queries, gt, ef)
         refgpu = None if args.no_ref_gpu else reference_gpu(base, adj, queries, gt, ef,
                                                             best["bf_words"], ids_op)
         use_learned = learned is not None and "qps" in learned and learned["qps"] > plain_qps
+        roof_learned = None
+        if learned is not None and "qps" in learned:
+            la = learned["algorithmic_bytes_per_launch"] / (learned["kernel_ms_avg"] / 1e3) / 1e9
+            lt, lsrc = ncu_traffic(learned["ef"], best["bf_words"], form="learned")
+            roof_learned = {
+                "kernel": "learned search_kernel<0,4,1,0,2> (entry + stop models)",
+                "bound": "hbm", "achieved": round(la, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(la / peak, 4), "peak_kind": peak_kind,
+                "traffic": lt, "traffic_source": lsrc,
+                "algorithmic_bytes_per_launch": learned["algorithmic_bytes_per_launch"],
+                "kernel_ms_avg": learned["kernel_ms_avg"],
+            }
         value = learned["qps"] if use_learned else plain_qps
         e2e_v = learned["e2e_qps"] if use_learned else plain_e2e
         out = {
@@ -464,14 +490,8 @@ def run_ours(args, ws, rank, local):
                     "h2d_bytes_per_step": int(queries.nbytes),
                     "d2h_bytes_per_step": int(NQ * K * (8 if use_learned else 4))},
             "gpu_launches": int(learned["gpu_launches"] if use_learned else plain_launches),
-            "roofline": {
-                "kernel": "plain search_kernel<0,4,1,0> at the plain operating point",
-                "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "traffic": traffic, "traffic_source": traffic_src,
-                "algorithmic_bytes_per_launch": round(launch_bytes),
-                "kernel_ms_avg": round(avg_kern_s * 1e3, 4),
-            },
+            "roofline": roof_learned if use_learned else roof_plain,
+            "roofline_plain": roof_plain,
             "serving": serving,
             "cpu_baseline": cpu,
             "reference_gpu_kernel": refgpu,

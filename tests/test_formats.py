@@ -57,3 +57,18 @@ def test_other_mixtures(ds):
     assert (g.base >= 0).all() and np.allclose(g.base.sum(1), 1.0, atol=1e-4)
     a = ds.angular_mixture(300, 10, dim=40, n_comp=4, seed=1)
     assert np.allclose(np.linalg.norm(a.base, axis=1), 1.0, atol=1e-4)
+
+
+def test_graph_file_roundtrip(ds, tmp_path):
+    adj = np.random.default_rng(1).integers(-1, 50, size=(50, 16)).astype(np.int32)
+    p = str(tmp_path / "g.song")
+    ds.save_graph(p, adj)
+    np.testing.assert_array_equal(ds.load_graph(p), adj)
+    raw = bytearray(open(p, "rb").read())
+    raw[-4:] = np.array([99], np.int32).tobytes()  # out-of-range neighbour
+    open(p, "wb").write(bytes(raw))
+    with pytest.raises(ValueError):
+        ds.load_graph(p)
+    open(p, "wb").write(b"not a graph file at all.")
+    with pytest.raises(ValueError):
+        ds.load_graph(p)
