@@ -7,6 +7,7 @@ calling the sm_100a kernels through the C ABI of ``include/song_b200.h``
 * :class:`Params`           -- config.h:9-58 as runtime values.
 * :class:`KernelGraph`      -- kernalGraph.h:20-71 (data + adj; ``upload_to_gpu``).
 * :class:`HashKernelGraph`  -- hashKernelGraph.h:22-126 (codes + adj).
+* :class:`BitHash`          -- bitHash.h:17-56, the projection on the GPU.
 * :func:`gpu_search`        -- kernalGraph.h:307-382 and the Hamming overload
   hashKernelGraph.h:360-435: returns the flat ``[nq*k]`` id list, best-first,
   ``-1`` padded, optionally filling a :class:`GpuSearchTrace`.
@@ -160,6 +161,11 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_server_run_poisson.argtypes = [vp, vp, ci, vp, vp, vp, C.c_double, C.c_uint, vp, vp,
                                           C.POINTER(C.c_double)]
     L.song_server_destroy.argtypes = [vp]
+    L.song_bithash_matrix.argtypes = [ci, ci, C.c_uint, vp]
+    L.song_bithash_project.argtypes = [vp, ci, ci, vp, i64, vp]
+    L.song_bithash_project_device.argtypes = [vp, ci, ci, vp, i64, i64, vp, i64, vp]
+    for name in ("song_bithash_matrix", "song_bithash_project", "song_bithash_project_device"):
+        getattr(L, name).restype = C.c_int
     for name in ("song_server_create", "song_server_submit", "song_server_poll",
                  "song_server_run_poisson", "song_server_destroy"):
         getattr(L, name).restype = C.c_int
@@ -316,6 +322,50 @@ class HashKernelGraph(_Index):
         _check(L.song_index_create_hamming(self.hashed.ctypes.data, self.num_nodes,
                                            self.hash_words, self.adj.ctypes.data,
                                            C.byref(self.params._c()), C.byref(self._h)))
+
+
+class BitHash:
+    """BitHash (bitHash.h:17-56): 1-bit Gaussian random projection to
+    ``hash_bits`` sign bits packed in u32 words.  The matrix ``R`` is drawn
+    exactly as the reference's constructor draws it (bitHash.h:23-27); the
+    projection runs on the GPU and is bit-identical to ``BitHash::project``
+    (sequential FP32 dot, separate multiply and add, ``dot > 0``)."""
+
+    def __init__(self, dim: int, seed: int = 42, hash_bits: int = 256):
+        self.dim = int(dim)
+        self.hash_bits = int(hash_bits)
+        self.R = np.empty((self.hash_bits, self.dim), np.float32)
+        _check(load_library().song_bithash_matrix(self.dim, self.hash_bits, int(seed),
+                                                  self.R.ctypes.data))
+
+    @property
+    def hash_words(self) -> int:  # HASH_WORDS, config.h:44
+        return self.hash_bits // 32
+
+    def project_all(self, data, n: Optional[int] = None) -> np.ndarray:
+        """bitHash.h:51-56: codes [n, hash_words] (u32) of data [n, dim]."""
+        x = np.ascontiguousarray(np.asarray(data, np.float32).reshape(-1, self.dim))
+        if n is not None:
+            x = x[:n]
+        out = np.empty((x.shape[0], self.hash_words), np.uint32)
+        _check(load_library().song_bithash_project(self.R.ctypes.data, self.dim, self.hash_bits,
+                                                   x.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    def project(self, vec) -> np.ndarray:
+        """bitHash.h:32-44: the code words of one vector."""
+        return self.project_all(np.asarray(vec, np.float32).reshape(1, self.dim))[0]
+
+    def project_device(self, d_R, d_x, n: int, d_codes, ldx: Optional[int] = None,
+                       ldc: Optional[int] = None, stream=None) -> None:
+        """project_all on device tensors (R as uploaded by the caller), async."""
+        def ptr(t):
+            return C.c_void_p(t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+        st = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        _check(load_library().song_bithash_project_device(
+            ptr(d_R), self.dim, self.hash_bits, ptr(d_x), int(n),
+            int(ldx if ldx is not None else self.dim), ptr(d_codes),
+            int(ldc if ldc is not None else self.hash_words), st))
 
 
 def build_graph(rows, params: Optional[Params] = None, kind: int = KIND_L2,

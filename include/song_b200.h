@@ -196,6 +196,29 @@ song_status song_build_graph_noalloc(int kind, const void* d_rows, int64_t n, in
                                      int build_bf_words, int32_t* d_adj, void* stream);
 
 /*
+ * BitHash (bitHash.h:17-56): sign-random-projection codes for the Hamming
+ * index.  song_bithash_matrix is the constructor BitHash(dim, seed)
+ * (bitHash.h:23-27): R[hash_bits x dim] (host, row-major) drawn from
+ * std::mt19937(seed) and std::normal_distribution<float>(0, 1), the same
+ * generator calls as the reference.  song_bithash_project is project_all
+ * (bitHash.h:51-56) on the GPU: codes[n x hash_bits/32] (host) with bit b of
+ * word w set when the FP32 dot of R[w*32+b] with x[i] is > 0, summed in
+ * increasing d with a separate multiply and add per step exactly as the
+ * reference's -O3 host build computes it, so the codes are bit-identical.
+ * hash_bits must be a positive multiple of 32 (HASH_WORDS = hash_bits/32,
+ * config.h:44).  Synchronous.
+ */
+song_status song_bithash_matrix(int dim, int hash_bits, unsigned seed, float* R);
+song_status song_bithash_project(const float* R, int dim, int hash_bits, const float* x,
+                                 int64_t n, uint32_t* codes);
+/* Device-pointer project_all: x[n x ldx] FP32 (ldx >= dim elements), R as
+ * above, codes[n x ldc] u32 (ldc >= hash_bits/32 words; words beyond
+ * hash_bits/32 are left untouched).  Asynchronous on `stream`. */
+song_status song_bithash_project_device(const float* d_R, int dim, int hash_bits,
+                                        const float* d_x, int64_t n, int64_t ldx,
+                                        uint32_t* d_codes, int64_t ldc, void* stream);
+
+/*
  * Attach a compressed copy of an L2 index's vectors for the precision form
  * (SONG_PREC_BF16 or SONG_PREC_FP8), converted on the GPU from the FP32
  * copy, which stays resident for the exact re-rank.  Replaces an earlier
