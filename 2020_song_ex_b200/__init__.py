@@ -161,6 +161,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_server_run_poisson.argtypes = [vp, vp, ci, vp, vp, vp, C.c_double, C.c_uint, vp, vp,
                                           C.POINTER(C.c_double)]
     L.song_server_destroy.argtypes = [vp]
+    L.song_index_u8_rows.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
+    L.song_index_u8_rows.restype = C.c_int
     L.song_bithash_matrix.argtypes = [ci, ci, C.c_uint, vp]
     L.song_bithash_project.argtypes = [vp, ci, ci, vp, i64, vp]
     L.song_bithash_project_device.argtypes = [vp, ci, ci, vp, i64, i64, vp, i64, vp]
@@ -301,6 +303,14 @@ class KernelGraph(_Index):
         _check(L.song_index_create_l2(self.data.ctypes.data, self.num_nodes, self.dim,
                                       self.adj.ctypes.data, C.byref(self.params._c()),
                                       C.byref(self._h)))
+
+    def u8_rows(self) -> int:
+        """Bytes per row of the exact byte copy of the rows (0 when the base is
+        not integer-valued in [0, 255]): the row size the plain and learned
+        searches gather for integer queries in [0, 255]."""
+        has, rb = C.c_int(), C.c_int()
+        _check(load_library().song_index_u8_rows(self._h, C.byref(has), C.byref(rb)))
+        return rb.value if has.value else 0
 
 
 class HashKernelGraph(_Index):

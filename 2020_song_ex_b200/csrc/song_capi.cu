@@ -54,6 +54,10 @@ struct song_index {
     float* d_dist = nullptr;
     size_t dist_cap = 0;
     // precision form: compressed copies of the FP32 rows
+    // integer rows in [0, 255]: an exact byte copy the plain search gathers
+    // instead of the FP32 rows (same distances, a quarter of the bytes)
+    uint8_t* d_u8 = nullptr;
+    int u8_ld = 0;  // bytes per row (multiple of 16)
     void* d_bf16 = nullptr;
     int bf16_ld = 0;  // bytes per row
     void* d_fp8 = nullptr;
@@ -137,6 +141,7 @@ void free_index(song_index* x) {
     cudaFree(x->d_ids);
     cudaFree(x->d_tr);
     cudaFree(x->d_dist);
+    cudaFree(x->d_u8);
     cudaFree(x->d_bf16);
     cudaFree(x->d_fp8);
     cudaFree(x->d_fp8_scale);
@@ -190,6 +195,15 @@ song_status create_common(int kind, const void* rows, int64_t n, int dim, const 
         e = cudaMemcpy(x->d_adj, adj, (size_t)n * params->block_size * sizeof(int32_t),
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(x->d_err, 0, 256);
+    if (e == cudaSuccess && kind == SONG_KIND_L2 && x->range.int_base && x->range.lo >= 0.0f &&
+        x->range.hi <= 255.0f && dim <= song::kU8MaxDim) {
+        x->u8_ld = song::u8_row_bytes(dim);
+        e = cudaMalloc(&x->d_u8, (size_t)n * x->u8_ld);
+        if (e == cudaSuccess)
+            e = song::convert_rows_u8((const float*)x->d_base, n, dim, x->ld, x->d_u8, x->u8_ld,
+                                      x->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
+    }
     if (e != cudaSuccess) {
         song_status s = cuda_fail(e, "index upload");
         free_index(x);
@@ -245,6 +259,8 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
     a->base_max = x->range.hi;
     a->out_dist = d_dist;
     a->qdim = x->dim;
+    a->u8 = x->d_u8;
+    a->u8_ld = x->u8_ld;
     const int prec = opts ? opts->precision : SONG_PREC_FP32;
     if (prec != SONG_PREC_FP32) {
         if (x->kind != SONG_KIND_L2)
@@ -478,6 +494,13 @@ song_status song_index_info(const song_index* x, int64_t* n, int* dim, int* kind
     if (n) *n = x->n;
     if (dim) *dim = x->dim;
     if (kind) *kind = x->kind;
+    return SONG_OK;
+}
+
+song_status song_index_u8_rows(const song_index* x, int* has_u8, int* row_bytes) {
+    if (!x) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (has_u8) *has_u8 = x->d_u8 != nullptr ? 1 : 0;
+    if (row_bytes) *row_bytes = x->u8_ld;
     return SONG_OK;
 }
 

@@ -32,8 +32,12 @@ struct SearchArgs {
     int n_multiprobe;        // N_MULTIPROBE
     int warp_smem;           // bytes of shared memory per warp (multiple of 16)
     int q_off, rows_off, cd_off, ci_off, rd_off, ri_off, bl_off;  // per-warp carve-up, bytes
+    int tm_cols;             // TMEM columns one CTA allocates (set by launch_search)
+    int tm_warp_cols;        // TMEM columns of one warp's queue ids (set by launch_search)
     int int_base;            // 1: every base value is an integer in [base_min, base_max]
     float base_min, base_max;
+    const uint8_t* u8;       // base values as bytes [n x u8_ld] when all are integers in [0, 255]
+    int u8_ld;               // bytes per byte row (multiple of 16)
     // precision form (prec != SONG_PREC_FP32)
     int prec;                // SONG_PREC_FP32 / SONG_PREC_BF16 / SONG_PREC_FP8
     const void* lowp;        // compressed rows [n x lowp_ld bytes]
@@ -81,6 +85,14 @@ struct BaseRange {
     float lo = 0.0f, hi = 0.0f;
 };
 BaseRange scan_base_range(const float* rows, int64_t n, int dim);
+
+// Byte rows of integer-valued vectors: at most kU8MaxDim elements, each row
+// zero padded to u8_row_bytes(dim) (a multiple of 16) -- the exact-integer
+// distance path then reads whole 16-byte chunks.
+constexpr int kU8MaxDim = 256;
+int u8_row_bytes(int dim);
+cudaError_t convert_rows_u8(const float* d_rows, int64_t n, int dim, int ld, uint8_t* d_out,
+                            int out_ld, cudaStream_t st);
 
 // Row stride (elements) the kernels use for `dim` elements of `kind`.
 int search_row_stride(int kind, int dim);

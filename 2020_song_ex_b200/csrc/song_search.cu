@@ -61,6 +61,8 @@ __constant__ uint64_t kBloomMix[8] = {
 
 __device__ __forceinline__ unsigned fbits(float x) { return __float_as_uint(x); }
 
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
 // Read-only loads of base rows (the read-only data path; an L1 no-allocate
 // variant measured slightly slower).
 __device__ __forceinline__ float ld_row(const float* p) { return __ldg(p); }
@@ -68,24 +70,75 @@ __device__ __forceinline__ float4 ld_row(const float4* p) { return __ldg(p); }
 __device__ __forceinline__ uint4 ld_row(const uint4* p) { return __ldg(p); }
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
-// Slot queue of capacity <= 1024 * GPL.  Slots live in shared memory; the
-// summary of group g (slots 32g .. 32g+31) is held by lane g % 32 in entry
-// g / 32.  Distances are non-negative, so their bit patterns order like the
-// floats.  All scalar fields are warp-uniform.
-template <int GPL>
+// Tensor memory (TMEM) access of one warp: 32 lanes x 32-bit columns.  The
+// wait is part of the same asm statement, so the loaded value is never used
+// before the load has completed, and a store has completed before the next
+// access of the same column.
+__device__ __forceinline__ unsigned tm_ld(uint32_t taddr) {
+    unsigned r;
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r)
+        : "r"(taddr)
+        : "memory");
+    return r;
+}
+__device__ __forceinline__ void tm_st(uint32_t taddr, unsigned v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};\n\t"
+        "tcgen05.wait::st.sync.aligned;"
+        :
+        : "r"(taddr), "r"(v)
+        : "memory");
+}
+
+// Slot queue of capacity <= 1024 * GPL.  Distances live in shared memory;
+// ids live in shared memory (TM = 0) or in the warp's 32 TMEM lanes, one
+// column per group of 32 slots, slot 32g + l at lane l of column tid + g
+// (TM = 1).  The summary of group g (slots 32g .. 32g+31) is held by lane
+// g % 32 in entry g / 32.  Distances are non-negative, so their bit patterns
+// order like the floats.  All scalar fields are warp-uniform.
+template <int GPL, int TM = 0>
 struct Queue {
     float* d;
-    int* id;
+    int* id;       // TM = 0
+    uint32_t tid;  // TM = 1: TMEM address of group 0's id column
     int sz;
     int cap;
     unsigned xb[GPL], xi[GPL];  // group maximum bits, first slot holding it (NONE = empty)
     unsigned nb[GPL], ni[GPL];  // group minimum bits, first slot holding it
 };
 
-template <int GPL>
-__device__ __forceinline__ void q_init(Queue<GPL>& q, float* d, int* id, int cap) {
+// Id of slot s (warp-uniform s; every lane gets it).
+template <int GPL, int TM>
+__device__ __forceinline__ int q_id(const Queue<GPL, TM>& q, int s) {
+    if constexpr (TM) {
+        const unsigned r = tm_ld(q.tid + (uint32_t)(s >> 5));
+        return (int)__shfl_sync(FULL, r, s & 31);
+    } else {
+        return q.id[s];
+    }
+}
+
+// Id of slot s := v (warp-uniform s and v; called by every lane).
+template <int GPL, int TM>
+__device__ __forceinline__ void q_set_id(Queue<GPL, TM>& q, int s, int v, int lane) {
+    if constexpr (TM) {
+        const uint32_t a = q.tid + (uint32_t)(s >> 5);
+        unsigned r = tm_ld(a);
+        if (lane == (s & 31)) r = (unsigned)v;
+        tm_st(a, r);
+    } else {
+        if (lane == 0) q.id[s] = v;
+    }
+}
+
+template <int GPL, int TM>
+__device__ __forceinline__ void q_init(Queue<GPL, TM>& q, float* d, int* id, uint32_t tid, int cap) {
     q.d = d;
     q.id = id;
+    q.tid = tid;
     q.sz = 0;
     q.cap = cap;
 #pragma unroll
@@ -98,8 +151,8 @@ __device__ __forceinline__ void q_init(Queue<GPL>& q, float* d, int* id, int cap
 }
 
 // Refresh the summary of group g from the slot array.  MIN: also the minimum.
-template <bool MIN, int GPL>
-__device__ __forceinline__ void group_update(Queue<GPL>& q, int g, int lane) {
+template <bool MIN, int GPL, int TM>
+__device__ __forceinline__ void group_update(Queue<GPL, TM>& q, int g, int lane) {
     const int s = (g << 5) + lane;
     const bool occ = s < q.sz;
     const unsigned b = occ ? fbits(q.d[s]) : 0u;
@@ -127,8 +180,8 @@ __device__ __forceinline__ void group_update(Queue<GPL>& q, int g, int lane) {
 }
 
 // First slot holding the maximum over [0, sz) (gpuHeap.h:29, :73, :83, :93).
-template <int GPL>
-__device__ __forceinline__ void root_max(const Queue<GPL>& q, unsigned& mb, unsigned& mi) {
+template <int GPL, int TM>
+__device__ __forceinline__ void root_max(const Queue<GPL, TM>& q, unsigned& mb, unsigned& mi) {
     unsigned b = 0u, i = NONE;
 #pragma unroll
     for (int r = 0; r < GPL; ++r)
@@ -141,8 +194,8 @@ __device__ __forceinline__ void root_max(const Queue<GPL>& q, unsigned& mb, unsi
 }
 
 // First slot holding the minimum over [0, sz) (gpuHeap.h:42, :263).
-template <int GPL>
-__device__ __forceinline__ void root_min(const Queue<GPL>& q, unsigned& mb, unsigned& mi) {
+template <int GPL, int TM>
+__device__ __forceinline__ void root_min(const Queue<GPL, TM>& q, unsigned& mb, unsigned& mi) {
     unsigned b = 0xffffffffu, i = NONE;
 #pragma unroll
     for (int r = 0; r < GPL; ++r)
@@ -156,13 +209,17 @@ __device__ __forceinline__ void root_min(const Queue<GPL>& q, unsigned& mb, unsi
 
 // Move the last slot into slot `hole` and shrink (the removal of
 // Candidates::pop_min, Results::pop_worst and drain_best).
-template <bool MIN, int GPL>
-__device__ __forceinline__ void q_remove(Queue<GPL>& q, int hole, int lane) {
+template <bool MIN, int GPL, int TM>
+__device__ __forceinline__ void q_remove(Queue<GPL, TM>& q, int hole, int lane) {
     const int last = q.sz - 1;
     __syncwarp();
-    if (lane == 0 && hole != last) {
-        q.d[hole] = q.d[last];
-        q.id[hole] = q.id[last];
+    if (hole != last) {
+        if (lane == 0) q.d[hole] = q.d[last];
+        if constexpr (TM) {
+            q_set_id(q, hole, q_id(q, last), lane);
+        } else {
+            if (lane == 0) q.id[hole] = q.id[last];
+        }
     }
     __syncwarp();
     q.sz = last;
@@ -172,9 +229,11 @@ __device__ __forceinline__ void q_remove(Queue<GPL>& q, int hole, int lane) {
 
 // Push (d, nb) of every lane in N, in lane order, with the semantics of
 // Candidates::push / Results::try_push (gpuHeap.h:23-36, :68-77).
-// Returns how many pushes were accepted.
-template <bool MIN, int GPL>
-__device__ __forceinline__ int q_push(Queue<GPL>& q, unsigned N, float d, int nb, int lane) {
+// Returns how many pushes were accepted.  `stage` (32 ints, TM = 1 only)
+// receives the ids in rank order for the column writes of an append.
+template <bool MIN, int GPL, int TM>
+__device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, int nb, int lane,
+                                      int* stage) {
     if (N == 0u) return 0;
     const bool mine = (N >> lane) & 1u;
     const int rank = __popc(N & lanemask_lt(lane));
@@ -185,10 +244,21 @@ __device__ __forceinline__ int q_push(Queue<GPL>& q, unsigned N, float d, int nb
         const int a = nm < room ? nm : room;
         if (mine && rank < a) {
             q.d[q.sz + rank] = d;
-            q.id[q.sz + rank] = nb;
+            if constexpr (TM) stage[rank] = nb;
+            else q.id[q.sz + rank] = nb;
         }
         __syncwarp();
         const int g0 = q.sz >> 5, g1 = (q.sz + a - 1) >> 5;
+        if constexpr (TM) {  // slots sz .. sz+a-1 take the staged ids, column by column
+            for (int g = g0; g <= g1; ++g) {
+                const uint32_t col = q.tid + (uint32_t)g;
+                unsigned r = tm_ld(col);
+                const int rr = (g << 5) + lane - q.sz;
+                if (rr >= 0 && rr < a) r = (unsigned)stage[rr];
+                tm_st(col, r);
+            }
+            __syncwarp();
+        }
         q.sz += a;
         for (int g = g0; g <= g1; ++g) group_update<MIN>(q, g, lane);
         acc = a;
@@ -201,10 +271,8 @@ __device__ __forceinline__ int q_push(Queue<GPL>& q, unsigned N, float d, int nb
             const int j = __ffs(rest) - 1;
             const float dj = __shfl_sync(FULL, d, j);
             const int nj = __shfl_sync(FULL, nb, j);
-            if (lane == 0) {
-                q.d[fi] = dj;
-                q.id[fi] = nj;
-            }
+            if (lane == 0) q.d[fi] = dj;
+            q_set_id(q, (int)fi, nj, lane);
             __syncwarp();
             group_update<MIN>(q, (int)(fi >> 5), lane);
             ++acc;
@@ -422,6 +490,73 @@ __device__ __forceinline__ float l2_int(const float* __restrict__ base, int ld,
     return out;
 }
 
+// Squared L2 of integer vectors in [0, 255] from their byte rows:
+// sum (q - b)^2 = sum q^2 + sum b^2 - 2 sum q*b, each term an exact unsigned
+// byte dot product (dp4a), so the result is the exact integer distance --
+// the same FP32 value the reference's float arithmetic produces, since all
+// of its partial sums are integers below 2^24 (dim <= 256).  Rows are read
+// in 16-byte chunks, 8 lanes per row, NC chunks per lane, 4 rows per pass
+// and two passes in flight; `qb` holds this lane's query chunks and `qq`
+// the query's sum of squares.
+template <int NC>
+__device__ __forceinline__ float l2_u8(const uint8_t* __restrict__ base, int ld, int nch,
+                                       const uint4 (&qb)[NC], int qq, int nb, unsigned N,
+                                       int* rows, int lane) {
+    const bool mine = (N >> lane) & 1u;
+    const int rank = __popc(N & lanemask_lt(lane));
+    const int m = __popc(N);
+    if (mine) rows[rank] = nb;
+    __syncwarp();
+    const int grp = lane >> 3, t = lane & 7;
+    float out = 0.0f;
+    for (int p0 = 0; p0 < m; p0 += 8) {
+        const int ra = p0 + grp, rb = p0 + 4 + grp;
+        const bool va = ra < m, vb = rb < m;
+        const uint4* pa = reinterpret_cast<const uint4*>(base + (size_t)(va ? rows[ra] : 0) * ld);
+        const uint4* pb = reinterpret_cast<const uint4*>(base + (size_t)(vb ? rows[rb] : 0) * ld);
+        uint4 xa[NC], xb[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int ch = t + 8 * c;
+            xa[c] = (va && ch < nch) ? ld_row(pa + ch) : make_uint4(0u, 0u, 0u, 0u);
+            xb[c] = (vb && ch < nch) ? ld_row(pb + ch) : make_uint4(0u, 0u, 0u, 0u);
+        }
+        unsigned qa = 0u, ba = 0u, qbb = 0u, bbb = 0u;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            qa = __dp4a(qb[c].x, xa[c].x, qa);
+            qa = __dp4a(qb[c].y, xa[c].y, qa);
+            qa = __dp4a(qb[c].z, xa[c].z, qa);
+            qa = __dp4a(qb[c].w, xa[c].w, qa);
+            ba = __dp4a(xa[c].x, xa[c].x, ba);
+            ba = __dp4a(xa[c].y, xa[c].y, ba);
+            ba = __dp4a(xa[c].z, xa[c].z, ba);
+            ba = __dp4a(xa[c].w, xa[c].w, ba);
+            qbb = __dp4a(qb[c].x, xb[c].x, qbb);
+            qbb = __dp4a(qb[c].y, xb[c].y, qbb);
+            qbb = __dp4a(qb[c].z, xb[c].z, qbb);
+            qbb = __dp4a(qb[c].w, xb[c].w, qbb);
+            bbb = __dp4a(xb[c].x, xb[c].x, bbb);
+            bbb = __dp4a(xb[c].y, xb[c].y, bbb);
+            bbb = __dp4a(xb[c].z, xb[c].z, bbb);
+            bbb = __dp4a(xb[c].w, xb[c].w, bbb);
+        }
+        int sa = (int)ba - 2 * (int)qa, sb = (int)bbb - 2 * (int)qbb;
+#pragma unroll
+        for (int w = 4; w >= 1; w >>= 1) {
+            sa += __shfl_xor_sync(FULL, sa, w);
+            sb += __shfl_xor_sync(FULL, sb, w);
+        }
+        // row of rank r sits in group r % 4 of pass r / 4
+        const int ga = __shfl_sync(FULL, sa, (rank & 3) << 3);
+        const int gb = __shfl_sync(FULL, sb, (rank & 3) << 3);
+        if (mine && (rank >> 2) == (p0 >> 2)) out = (float)(qq + ga);
+        if (mine && (rank >> 2) == (p0 >> 2) + 1) out = (float)(qq + gb);
+    }
+    __syncwarp();
+    return out;
+}
+
 // Hamming distance of this lane's own row: popcount(q ^ b) over W4 uint4
 // (warp_hamming, hashKernelGraph.h:215-224; integer, so order-free).
 template <int W4>
@@ -445,15 +580,17 @@ __device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int
 // extracted first (into the free candidate arrays); if their distances are
 // strictly increasing the replay's outcome is exactly those k in order.
 // Otherwise the extraction is undone and the trims and drains are replayed.
-template <int GPL>
-__device__ __forceinline__ int finish(Queue<GPL>& res, Queue<GPL>& cand, int k, int32_t* out,
-                                      float* outd, int lane) {
+// `scratch` (TM = 1: at least cap ints of shared memory) holds the slots of
+// the extracted results; with TM = 0 the free candidate id array does.
+template <int GPL, int TM>
+__device__ __forceinline__ int finish(Queue<GPL, TM>& res, Queue<GPL, TM>& cand, int k,
+                                      int32_t* out, float* outd, int lane, int* scratch) {
     const int ng = (res.sz + 31) >> 5;
     for (int g = 0; g < ng; ++g) group_update<true>(res, g, lane);
     const int cnt = res.sz < k ? res.sz : k;
     const int take = res.sz < k + 1 ? res.sz : k + 1;
     unsigned* xv = reinterpret_cast<unsigned*>(cand.d);  // extracted distance bits
-    int* xs = cand.id;                                   // their slots
+    int* xs = TM ? scratch : cand.id;                    // their slots
     for (int i = 0; i < take; ++i) {
         unsigned mb, mi;
         root_min(res, mb, mi);
@@ -469,9 +606,18 @@ __device__ __forceinline__ int finish(Queue<GPL>& res, Queue<GPL>& cand, int k, 
     for (int i = lane; i + 1 < take; i += 32) distinct &= xv[i] < xv[i + 1];
     distinct = __all_sync(FULL, distinct);
     if (distinct) {
-        for (int i = lane; i < cnt; i += 32) {
-            out[i] = res.id[xs[i]];
-            if (outd) outd[i] = __uint_as_float(xv[i]);
+        if constexpr (TM) {
+            for (int i = 0; i < cnt; ++i) {
+                const int id = q_id(res, xs[i]);
+                if (lane == (i & 31)) out[i] = id;
+            }
+            for (int i = lane; i < cnt; i += 32)
+                if (outd) outd[i] = __uint_as_float(xv[i]);
+        } else {
+            for (int i = lane; i < cnt; i += 32) {
+                out[i] = res.id[xs[i]];
+                if (outd) outd[i] = __uint_as_float(xv[i]);
+            }
         }
     } else {
         for (int i = lane; i < take; i += 32) reinterpret_cast<unsigned*>(res.d)[xs[i]] = xv[i];
@@ -485,7 +631,7 @@ __device__ __forceinline__ int finish(Queue<GPL>& res, Queue<GPL>& cand, int k, 
         for (int i = 0; i < cnt; ++i) {  // Results::drain_best
             unsigned mb, mi;
             root_min(res, mb, mi);
-            const int id = res.id[mi];
+            const int id = q_id(res, (int)mi);
             if (lane == 0) {
                 out[i] = id;
                 if (outd) outd[i] = __uint_as_float(mb);
@@ -589,20 +735,28 @@ __device__ __forceinline__ float l2_lowp(const SearchArgs& a, const float* sq, i
 // Precision form, final step: exact FP32 distances of every entry of the
 // results queue (FP32 rows, 8 lanes per row), then the k smallest by
 // (distance, id) in ascending order, -1 padded.
-template <int GPL>
-__device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL>& res,
-                                             Queue<GPL>& cand, const float* sq, int32_t* out,
+template <int GPL, int TM>
+__device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL, TM>& res,
+                                             Queue<GPL, TM>& cand, const float* sq, int32_t* out,
                                              float* outd, int lane) {
     const int m = res.sz;
     float* rd = cand.d;
-    int* rid = cand.id;
+    int* rid = cand.id;  // TM = 0 only; with TM = 1 the ids stay in res's TMEM columns
     const float* base = reinterpret_cast<const float*>(a.base);
     const int nch = a.ld >> 2;  // float4 per FP32 row
     const int grp = lane >> 3, t = lane & 7;
+    unsigned gid = 0;  // TM = 1: ids of the current group, lane l = slot 32g + l
     for (int p0 = 0; p0 < m; p0 += 4) {
         const int r = p0 + grp;
         const bool v = r < m;
-        const int id = v ? res.id[r] : 0;
+        int id;
+        if constexpr (TM) {
+            if ((p0 & 31) == 0) gid = tm_ld(res.tid + (uint32_t)(p0 >> 5));
+            id = (int)__shfl_sync(FULL, gid, r & 31);
+            if (!v) id = 0;
+        } else {
+            id = v ? res.id[r] : 0;
+        }
         const float4* row = reinterpret_cast<const float4*>(base + (size_t)id * a.ld);
         float acc = 0.0f;
         for (int c = t; c < nch; c += 8) {
@@ -621,19 +775,24 @@ __device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL>& re
         for (int w = 4; w >= 1; w >>= 1) acc += __shfl_xor_sync(FULL, acc, w);
         if (t == 0 && v) {
             rd[r] = acc;
-            rid[r] = id;
+            if constexpr (!TM) rid[r] = id;
         }
     }
     __syncwarp();
     const int cnt = m < a.k ? m : a.k;
     for (int i = 0; i < cnt; ++i) {
         unsigned bb = 0xffffffffu, bi = 0xffffffffu;
-        for (int s2 = lane; s2 < m; s2 += 32) {
-            const unsigned b = fbits(rd[s2]);
-            const unsigned id = (unsigned)rid[s2];
-            if (b < bb || (b == bb && id < bi)) {
-                bb = b;
-                bi = id;
+        for (int s0 = 0; s0 < m; s0 += 32) {  // warp-uniform trip count (TMEM loads are collective)
+            const int s2 = s0 + lane;
+            unsigned id;
+            if constexpr (TM) id = tm_ld(res.tid + (uint32_t)(s0 >> 5));
+            else id = s2 < m ? (unsigned)rid[s2] : 0u;
+            if (s2 < m) {
+                const unsigned b = fbits(rd[s2]);
+                if (b < bb || (b == bb && id < bi)) {
+                    bb = b;
+                    bi = id;
+                }
             }
         }
         const unsigned mb = __reduce_min_sync(FULL, bb);
@@ -642,8 +801,13 @@ __device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL>& re
             out[i] = (int)mi;
             if (outd) outd[i] = __uint_as_float(mb);
         }
-        for (int s2 = lane; s2 < m; s2 += 32)  // taken: out of every later minimum
-            if ((unsigned)rid[s2] == mi) rd[s2] = __uint_as_float(0xffffffffu);
+        for (int s0 = 0; s0 < m; s0 += 32) {  // taken: out of every later minimum
+            const int s2 = s0 + lane;
+            unsigned id;
+            if constexpr (TM) id = tm_ld(res.tid + (uint32_t)(s0 >> 5));
+            else id = s2 < m ? (unsigned)rid[s2] : 0u;
+            if (s2 < m && id == mi) rd[s2] = __uint_as_float(0xffffffffu);
+        }
         __syncwarp();
     }
     for (int i = cnt + lane; i < a.k; i += 32) {
@@ -797,12 +961,18 @@ __device__ __forceinline__ unsigned fkey(float x) {
 // KIND 1 = Hamming with NE uint4 of code per row.  GPL: queue groups per lane.
 // DT: SONG_PREC_FP32 (the plain, bit-exact search) or the precision form on
 // BF16 / FP8 rows (KIND 0, query in shared memory, FP32 re-rank at the end).
-template <int KIND, int NE, int GPL, int DT, int LM>
+// TM = 1: the queue ids live in this warp's TMEM lanes from column `tbase`
+// (candidates in columns tbase .. tbase+G-1, results in the next G, with G =
+// ceil(cap / 32)); the per-warp shared-memory layout then has no id arrays.
+template <int KIND, int NE, int GPL, int DT, int LM, int TM = 0>
 __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsigned char* ws,
-                                             int lane) {
-    Queue<GPL> cand, res;
-    q_init(cand, reinterpret_cast<float*>(ws + a.cd_off), reinterpret_cast<int*>(ws + a.ci_off), a.cap);
-    q_init(res, reinterpret_cast<float*>(ws + a.rd_off), reinterpret_cast<int*>(ws + a.ri_off), a.cap);
+                                             int lane, uint32_t tbase = 0) {
+    Queue<GPL, TM> cand, res;
+    const uint32_t ngrp = (uint32_t)((a.cap + 31) >> 5);
+    q_init(cand, reinterpret_cast<float*>(ws + a.cd_off), reinterpret_cast<int*>(ws + a.ci_off),
+           tbase, a.cap);
+    q_init(res, reinterpret_cast<float*>(ws + a.rd_off), reinterpret_cast<int*>(ws + a.ri_off),
+           tbase + ngrp, a.cap);
     uint64_t* bloom = reinterpret_cast<uint64_t*>(ws + a.bl_off);
     float* sq = reinterpret_cast<float*>(ws + a.q_off);
     int* rows = reinterpret_cast<int*>(ws + a.rows_off);
@@ -816,10 +986,13 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 
     // Query in registers (and shared memory for the generic L2 path).
     constexpr bool kIntPath = KIND == 0 && NE > 0 && DT == SONG_PREC_FP32;
+    constexpr int kNC = NE >= 8 ? 2 : 1;  // 16-byte query chunks per lane on the byte-row path
     float qreg[(KIND == 0 && NE > 0) ? NE : 1];
     float4 qv[kIntPath ? NE : 1];
+    uint4 qb[kIntPath ? kNC : 1];
     uint4 qcode[KIND == 1 ? NE : 1];
-    bool int_exact = false;
+    bool int_exact = false, u8_mode = false;
+    int qq = 0;
     if constexpr (KIND == 0) {
         const float* qg = reinterpret_cast<const float*>(a.queries) + (int64_t)qid * a.qld;
         if constexpr (NE > 0) {
@@ -835,7 +1008,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     integral &= qreg[e] == rintf(qreg[e]);
                 }
             }
-            if (a.int_base && a.dim == 32 * NE) {
+            if (a.int_base && (a.dim == 32 * NE || a.u8 != nullptr)) {
                 // every |q_i - b_i| <= maxd; dim * maxd^2 < 2^24 keeps all sums exact
                 integral = __all_sync(FULL, integral);
 #pragma unroll
@@ -845,7 +1018,37 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 }
                 const double maxd = fmax((double)a.base_max - lo, (double)hi - a.base_min);
                 int_exact = integral && (double)a.dim * maxd * maxd < 16777216.0;
-                if (int_exact) {
+                // byte rows (base in [0, 255]) and a query in [0, 255]: exact dp4a distances
+                u8_mode = kIntPath && int_exact && a.u8 != nullptr && lo >= 0.0f && hi <= 255.0f;
+                if (u8_mode) {
+                    int s2 = 0;
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) {
+                        const int v = (int)qreg[e];  // zero beyond dim
+                        s2 += v * v;
+                    }
+                    qq = (int)__reduce_add_sync(FULL, (unsigned)s2);
+#pragma unroll
+                    for (int c = 0; c < kNC; ++c) {  // lane t of 8: bytes 16(t + 8c) .. +15
+                        const int e0 = 16 * ((lane & 7) + 8 * c);
+                        unsigned w4[4];
+#pragma unroll
+                        for (int wd = 0; wd < 4; ++wd) {
+                            unsigned wv = 0u;
+#pragma unroll
+                            for (int bt = 0; bt < 4; ++bt) {
+                                const int e = e0 + 4 * wd + bt;
+                                const unsigned bv = e < a.dim ? (unsigned)__ldcg(qg + e) : 0u;
+                                wv |= bv << (8 * bt);
+                            }
+                            w4[wd] = wv;
+                        }
+                        qb[c] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                    }
+                } else if (int_exact && a.dim != 32 * NE) {
+                    int_exact = false;  // the float4 gather path needs dim == 32 * NE
+                }
+                if (int_exact && !u8_mode) {
                     const float4* q4 = reinterpret_cast<const float4*>(qg);
                     const bool aligned = ((reinterpret_cast<uintptr_t>(qg) & 15u) == 0);
 #pragma unroll
@@ -881,7 +1084,8 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         } else if constexpr (KIND == 0) {
             const float* base = reinterpret_cast<const float*>(a.base);
             if constexpr (kIntPath) {
-                if (int_exact) d = l2_int<NE>(base, a.ld, qv, nb, N, rows, lane);
+                if (u8_mode) d = l2_u8<kNC>(a.u8, a.u8_ld, a.u8_ld >> 4, qb, qq, nb, N, rows, lane);
+                else if (int_exact) d = l2_int<NE>(base, a.ld, qv, nb, N, rows, lane);
                 else d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
             } else {
                 d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
@@ -942,7 +1146,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             unsigned mb, mi;
             root_min(cand, mb, mi);
             const float cmin = __uint_as_float(mb);
-            const int cn = cand.id[mi];
+            const int cn = q_id(cand, (int)mi);
             limit = a.block_size;
             arow = a.adj + (int64_t)cn * a.block_size;
             q_remove<true>(cand, (int)mi, lane);
@@ -1007,8 +1211,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             if (cand.sz > 0) {  // the next pop is most often today's runner-up: warm its row in L2
                 unsigned nb2, ni2;
                 root_min(cand, nb2, ni2);
+                const int nid = q_id(cand, (int)ni2);
                 if (lane == 0) {
-                    const int32_t* nrow = a.adj + (int64_t)cand.id[ni2] * a.block_size;
+                    const int32_t* nrow = a.adj + (int64_t)nid * a.block_size;
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(nrow));
                 }
             }
@@ -1040,8 +1245,8 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             }
             tr.visited_nodes += c;
             tr.distance_evals += c;
-            const int pf = q_push<true>(cand, N, d, nb, lane);
-            const int pr = q_push<false>(res, N, d, nb, lane);
+            const int pf = q_push<true>(cand, N, d, nb, lane, rows);
+            const int pr = q_push<false>(res, N, d, nb, lane, rows);
             tr.frontier_pushes += pf;
             tr.result_updates += pr;
             if constexpr (LM > 0) {
@@ -1074,46 +1279,116 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     if (DT != SONG_PREC_FP32 && a.rerank)
         tr.result_count = rerank_finish(a, res, cand, sq, a.out + (int64_t)qid * a.k, outd, lane);
     else
-        tr.result_count = finish(res, cand, a.k, a.out + (int64_t)qid * a.k, outd, lane);
+        tr.result_count = finish(res, cand, a.k, a.out + (int64_t)qid * a.k, outd, lane,
+                                 reinterpret_cast<int*>(bloom));
     if (a.trace != nullptr && lane == 0) a.trace[qid] = tr;
 }
 
 #include "song_serve_kernel.inc"
 
+// Launch shape of a search_kernel instance.  Queues of up to 1024 slots keep
+// their ids in TMEM (TM): CTAs of 4 warps, one warp per TMEM lane quarter,
+// and at most 80 registers per thread so that 6 CTAs (24 warps) fit an SM --
+// the search is latency-bound and gains from every resident query.  The
+// learned-model and 256-float-query instances hold more live state; they
+// get 96 registers (5 CTAs, 20 warps) instead of spilling.  Larger queues
+// keep the ids in shared memory, up to 8 warps per CTA.
+template <int KIND, int NE, int GPL, int DT, int LM>
+struct KernelShape {
+    static constexpr int kTM = GPL == 1 ? 1 : 0;
+    static constexpr int kThreads = kTM ? 128 : 256;
+    static constexpr int kMinBlocks = kTM ? ((LM > 0 || NE >= 8) ? 5 : 6) : 1;
+    static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
+};
+
 template <int KIND, int NE, int GPL, int DT, int LM = 0>
-__global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
+__global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads),
+                                  (KernelShape<KIND, NE, GPL, DT, LM>::kMinBlocks))
+    search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
-    unsigned char* ws = smem + (size_t)(threadIdx.x >> 5) * a.warp_smem;
+    constexpr int TM = KernelShape<KIND, NE, GPL, DT, LM>::kTM;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char* ws = smem + (size_t)warp * a.warp_smem;
+    uint32_t tbase = 0;
+    __shared__ uint32_t tm_slot;
+    if constexpr (TM) {  // one TMEM allocation per CTA, warp w uses lanes 32(w%4) .. +31
+        if (warp == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                         :: "r"((uint32_t)__cvta_generic_to_shared(&tm_slot)), "r"(a.tm_cols)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        tbase = tm_slot + ((uint32_t)(32 * (warp & 3)) << 16) +
+                (uint32_t)((warp >> 2) * a.tm_warp_cols);
+    }
     for (;;) {
         int qid = 0;
         if (lane == 0) qid = (int)atomicAdd(a.counter, 1u);
         qid = __shfl_sync(FULL, qid, 0);
         if (qid >= a.nq) break;
-        search_query<KIND, NE, GPL, DT, LM>(a, qid, ws, lane);
+        search_query<KIND, NE, GPL, DT, LM, TM>(a, qid, ws, lane, tbase);
+    }
+    if constexpr (TM) {  // every warp is done with TMEM before it is freed
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (warp == 0)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                         :: "r"(tm_slot), "r"(a.tm_cols) : "memory");
     }
 }
 
 using KernelFn = void (*)(const SearchArgs);
 
+// A chosen kernel instance and its launch shape.
+struct KernelSel {
+    KernelFn fn = nullptr;
+    int tm = 0;
+    int threads = 256;
+    bool query_smem = true;
+};
+
+template <int KIND, int NE, int GPL, int DT, int LM = 0>
+KernelSel ksel() {
+    using S = KernelShape<KIND, NE, GPL, DT, LM>;
+    KernelSel k;
+    k.fn = search_kernel<KIND, NE, GPL, DT, LM>;
+    k.tm = S::kTM;
+    k.threads = S::kThreads;
+    k.query_smem = S::kQuerySmem;
+    return k;
+}
+
 template <int GPL>
-KernelFn pick_gpl(int kind, const SearchArgs& a) {
+KernelSel pick_gpl(int kind, const SearchArgs& a) {
     if (kind == SONG_KIND_L2) {
-        if (a.prec == SONG_PREC_BF16) return search_kernel<0, 0, GPL, SONG_PREC_BF16>;
-        if (a.prec == SONG_PREC_FP8) return search_kernel<0, 0, GPL, SONG_PREC_FP8>;
-        if (a.dim <= 32) return search_kernel<0, 1, GPL, 0>;
-        if (a.dim <= 64) return search_kernel<0, 2, GPL, 0>;
-        if (a.dim <= 128) return search_kernel<0, 4, GPL, 0>;
-        if (a.dim <= 256) return search_kernel<0, 8, GPL, 0>;
-        return search_kernel<0, 0, GPL, 0>;
+        if (a.prec == SONG_PREC_BF16) return ksel<0, 0, GPL, SONG_PREC_BF16>();
+        if (a.prec == SONG_PREC_FP8) return ksel<0, 0, GPL, SONG_PREC_FP8>();
+        if (a.dim <= 32) return ksel<0, 1, GPL, 0>();
+        if (a.dim <= 64) return ksel<0, 2, GPL, 0>();
+        if (a.dim <= 128) return ksel<0, 4, GPL, 0>();
+        if (a.dim <= 256) return ksel<0, 8, GPL, 0>();
+        return ksel<0, 0, GPL, 0>();
     }
     switch (a.ld) {
-        case 4: return search_kernel<1, 1, GPL, 0>;
-        case 8: return search_kernel<1, 2, GPL, 0>;
-        case 16: return search_kernel<1, 4, GPL, 0>;
-        case 32: return search_kernel<1, 8, GPL, 0>;
-        default: return nullptr;
+        case 4: return ksel<1, 1, GPL, 0>();
+        case 8: return ksel<1, 2, GPL, 0>();
+        case 16: return ksel<1, 4, GPL, 0>();
+        case 32: return ksel<1, 8, GPL, 0>();
+        default: return KernelSel();
     }
+}
+
+// FP32 rows of integers in [0, 255] -> byte rows, zero padded to out_ld bytes.
+__global__ void rows_to_u8(const float* __restrict__ x, int64_t n, int dim, int ld,
+                           uint8_t* __restrict__ out, int out_ld) {
+    const int64_t r = blockIdx.x;
+    if (r >= n) return;
+    for (int i = threadIdx.x; i < out_ld; i += blockDim.x)
+        out[r * out_ld + i] = i < dim ? (uint8_t)x[r * ld + i] : (uint8_t)0;
 }
 
 // FP32 -> BF16 (round to nearest even) rows, zero padded to out_ld bytes.
@@ -1150,27 +1425,81 @@ __global__ void quantize_fp8(const float* __restrict__ x, int64_t n, int dim, in
 }
 
 template <int LM>
-KernelFn pick_learned(const SearchArgs& a) {
-    if (a.prec == SONG_PREC_BF16) return search_kernel<0, 0, 1, SONG_PREC_BF16, LM>;
-    if (a.prec == SONG_PREC_FP8) return search_kernel<0, 0, 1, SONG_PREC_FP8, LM>;
-    if (a.dim <= 128 && a.dim > 64) return search_kernel<0, 4, 1, 0, LM>;
-    return search_kernel<0, 0, 1, 0, LM>;
+KernelSel pick_learned(const SearchArgs& a) {
+    if (a.prec == SONG_PREC_BF16) return ksel<0, 0, 1, SONG_PREC_BF16, LM>();
+    if (a.prec == SONG_PREC_FP8) return ksel<0, 0, 1, SONG_PREC_FP8, LM>();
+    if (a.dim <= 128 && a.dim > 64) return ksel<0, 4, 1, 0, LM>();
+    return ksel<0, 0, 1, 0, LM>();
 }
 
-KernelFn pick_kernel(int kind, const SearchArgs& a) {
+KernelSel pick_kernel(int kind, const SearchArgs& a) {
     if (a.lm != 0) {  // learned entry/stop: L2, queues up to 1024 slots
-        if (kind != SONG_KIND_L2 || a.cap > 1024) return nullptr;
+        if (kind != SONG_KIND_L2 || a.cap > 1024) return KernelSel();
         return a.lm == 1 ? pick_learned<1>(a) : pick_learned<2>(a);
     }
     if (a.cap <= 1024) return pick_gpl<1>(kind, a);
     if (a.cap <= 2048) return pick_gpl<2>(kind, a);
     if (a.cap <= 4096) return pick_gpl<4>(kind, a);
-    return nullptr;
+    return KernelSel();
 }
 
-int round_up(int x, int m) { return (x + m - 1) / m * m; }
+// Resident CTAs per SM of a TMEM-id kernel.  The runtime's occupancy query
+// reports a single CTA per SM for kernels that allocate tensor memory, yet
+// several such CTAs run side by side when their registers, shared memory and
+// TMEM columns fit, so the limit is computed from those resources: registers
+// are allocated per warp in units of 8 per thread out of 16,384 per SM
+// sub-partition (four per SM), shared memory per CTA includes the runtime's
+// reservation, and each SM has 512 TMEM columns.  A CTA beyond what fits
+// would only wait in tcgen05.alloc for an earlier one to finish.
+cudaError_t tm_ctas_per_sm(KernelFn fn, int dev, int warps, size_t dyn_smem, int tm_cols, int* out) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess) return e;
+    int smem_sm = 0, reserved = 0, regs_sm = 0, max_blocks = 0, max_threads = 0;
+    e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_blocks, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_threads, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    if (e != cudaSuccess) return e;
+    const size_t cta_smem = dyn_smem + fa.sharedSizeBytes + (size_t)reserved;
+    const int by_smem = (int)((size_t)smem_sm / cta_smem);
+    const int warp_regs = ((fa.numRegs + 7) / 8) * 8 * 32;
+    const int warps_per_quarter = warp_regs > 0 ? (regs_sm / 4) / warp_regs : 64;
+    const int by_regs = (warps_per_quarter * 4) / warps;
+    const int by_threads = max_threads / (warps * 32);
+    const int by_tmem = 512 / tm_cols;
+    *out = std::min(std::min(std::min(by_smem, by_regs), std::min(by_threads, max_blocks)), by_tmem);
+    return cudaSuccess;
+}
+
+// Per-warp shared memory of the TMEM-id kernels: [query if kept in shared
+// memory][32-entry row list][candidate distances][result distances][Bloom
+// filter], the Bloom region being at least cap ints because finish() keeps
+// the extracted slots there once the search is over.
+void tm_layout(int query_floats, SearchArgs* a) {
+    const int capr = round_up(a->cap, 32);
+    a->q_off = 0;
+    a->rows_off = round_up(query_floats * 4, 16);
+    a->cd_off = a->rows_off + 128;
+    a->rd_off = a->cd_off + capr * 4;
+    a->ci_off = 0;
+    a->ri_off = 0;
+    a->bl_off = round_up(a->rd_off + capr * 4, 16);
+    a->warp_smem = round_up(a->bl_off + std::max(a->bf_words * 8, capr * 4), 16);
+    a->tm_warp_cols = 2 * (capr / 32);
+}
 
 }  // namespace
+
+int u8_row_bytes(int dim) { return round_up(dim, 16); }
+
+cudaError_t convert_rows_u8(const float* d_rows, int64_t n, int dim, int ld, uint8_t* d_out,
+                            int out_ld, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    rows_to_u8<<<(unsigned)n, 128, 0, st>>>(d_rows, n, dim, ld, d_out, out_ld);
+    return cudaGetLastError();
+}
 
 int search_row_stride(int kind, int dim) {
     if (kind == SONG_KIND_L2) return round_up(dim, 4);
@@ -1245,26 +1574,44 @@ cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStre
     return cudaGetLastError();
 }
 
-cudaError_t launch_search(int kind, const SearchArgs& a, int num_sms, cudaStream_t stream) {
-    if (a.nq <= 0) return cudaSuccess;
-    KernelFn fn = pick_kernel(kind, a);
-    if (fn == nullptr) return cudaErrorInvalidValue;
+cudaError_t launch_search(int kind, const SearchArgs& args, int num_sms, cudaStream_t stream) {
+    if (args.nq <= 0) return cudaSuccess;
+    const KernelSel ks = pick_kernel(kind, args);
+    if (ks.fn == nullptr) return cudaErrorInvalidValue;
+    KernelFn fn = ks.fn;
+    SearchArgs a = args;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     int smem_optin = 0;
     e = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
-    // Up to 8 warps per CTA while the CTA's shared memory stays within a
-    // quarter of the opt-in limit, so several CTAs can share an SM.
-    int warps = 8;
-    while (warps > 1 && (size_t)warps * a.warp_smem > (size_t)smem_optin / 4) warps >>= 1;
+    int warps;
+    if (ks.tm) {
+        // ids in TMEM: CTAs of 4 warps, one per lane quarter; 2 * ceil(cap/32)
+        // columns per warp, allocated per CTA in a power of two >= 32
+        tm_layout(ks.query_smem ? a.qdim : 0, &a);
+        warps = ks.threads / 32;
+        int cols = 32;
+        while (cols < a.tm_warp_cols * (warps / 4)) cols <<= 1;
+        if (cols > 512) return cudaErrorInvalidConfiguration;
+        a.tm_cols = cols;
+    } else {
+        // Up to 8 warps per CTA while the CTA's shared memory stays within a
+        // quarter of the opt-in limit, so several CTAs can share an SM.
+        warps = 8;
+        while (warps > 1 && (size_t)warps * a.warp_smem > (size_t)smem_optin / 4) warps >>= 1;
+    }
     const size_t smem = (size_t)warps * a.warp_smem;
     if (smem > (size_t)smem_optin) return cudaErrorInvalidConfiguration;
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, warps * 32, smem);
+    if (ks.tm) {
+        e = tm_ctas_per_sm(fn, dev, warps, smem, a.tm_cols, &per_sm);
+    } else {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, warps * 32, smem);
+    }
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int64_t need = ((int64_t)a.nq + warps - 1) / warps;

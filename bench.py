@@ -52,7 +52,7 @@ SEED = 2020
 BLOCK_SIZE = 32
 TARGET_RECALL = 0.95
 EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 512, 640, 768, 1024)
-BF_SWEEP = (256, 1024)
+BF_SWEEP = (256, 512, 1024)
 LEARN_THRESHOLDS = (0.8, 0.85, 0.9, 0.95, 0.98)
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
 
@@ -163,11 +163,13 @@ def ncu_traffic(ef: int, bf_words: int, form: str = "plain"):
     return None, None
 
 
-def bytes_per_query(trace: np.ndarray, k: int) -> np.ndarray:
-    """Algorithmic bytes: E*dim*4 + X*BLOCK_SIZE*4 + dim*4 + k*4 per query."""
+def bytes_per_query(trace: np.ndarray, k: int, row_bytes: int = DIM * 4) -> np.ndarray:
+    """Algorithmic bytes: E*row + X*BLOCK_SIZE*4 + dim*4 + k*4 per query, where
+    row is the bytes of one gathered vector: dim*4 for FP32 rows, or the byte
+    row (dim rounded up to 16) that integer vectors in [0, 255] are read from."""
     E = trace[:, 5].astype(np.float64)
     X = trace[:, 2].astype(np.float64)
-    return E * DIM * 4 + X * BLOCK_SIZE * 4 + DIM * 4 + k * 4
+    return E * row_bytes + X * BLOCK_SIZE * 4 + DIM * 4 + k * 4
 
 
 def _gpu_index(local: int) -> int:
@@ -295,7 +297,8 @@ def run_ours(args, ws, rank, local):
     trace = d_tr.cpu().numpy()
     ids_op = d_ids.cpu().numpy()
     recall = float(ds.recall_at_k(ids_op, gt, K).mean())
-    launch_bytes = float(bytes_per_query(trace, K).sum())
+    row_bytes = g.u8_rows() or DIM * 4  # the bench vectors and queries are integers in [0, 255]
+    launch_bytes = float(bytes_per_query(trace, K, row_bytes).sum())
 
     parity = None
     if rank == 0 and not args.no_parity:  # bit-exactness at full size (oracle = checker)
@@ -384,7 +387,8 @@ def run_ours(args, ws, rank, local):
             ids_l = d_ids.cpu().numpy()
             song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
             stream.synchronize()
-            l_bytes = float(bytes_per_query(d_tr.cpu().numpy(), K).sum())
+            l_bytes = float(bytes_per_query(d_tr.cpu().numpy(), K,
+                                            row_bytes if lprec == song.PREC_FP32 else DIM * 2).sum())
             copts = lopts._c()
 
             def host_learned():

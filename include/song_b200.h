@@ -135,6 +135,17 @@ song_status song_index_destroy(song_index* index);
 song_status song_index_info(const song_index* index, int64_t* n, int* dim, int* kind);
 
 /*
+ * Whether an L2 index keeps a byte copy of its rows (no counterpart in the
+ * reference).  When every base value is an integer in [0, 255] (and dim <=
+ * 256) the index stores the rows also as bytes, row_bytes each; the plain and
+ * learned searches then compute the distances of queries whose values are
+ * integers in [0, 255] from those bytes, exactly (the same FP32 distances as
+ * the reference's float arithmetic, which is exact for such vectors), and
+ * gather a quarter of the bytes.
+ */
+song_status song_index_u8_rows(const song_index* index, int* has_u8, int* row_bytes);
+
+/*
  * gpu_search (kernalGraph.h:307-382): host queries[nq x dim] in, host
  * ids[nq x k] out (best-first, -1 padded).  ef_search is clamped exactly as
  * the reference does (raise to k, then cap at pq_size).  traces (host,

@@ -169,3 +169,36 @@ def test_empty_and_zero_k(cuda, song):
     assert song.gpu_search(g, np.zeros((0, 8), np.float32), 0, 10).size == 0
     assert song.gpu_search(g, np.zeros((3, 8), np.float32), 3, 0).size == 0
     g.close()
+
+
+@pytest.mark.parametrize("dim", [128, 200, 37])
+def test_byte_rows_and_their_fallbacks(cuda, song, ds, oracle, dim):
+    """Integer rows in [0, 255] get an exact byte copy; queries in [0, 255]
+    use it, queries outside that range (but integral) and non-integral
+    queries fall back to the FP32 rows -- all bit-exact with the oracle,
+    including the QueryTrace counters, in one batch."""
+    base, q = _case(ds, "int", 2500, 90, dim, seed=dim + 7)
+    q = q.copy()
+    q[30:45, 0] = 300.0                   # integral, outside the byte range
+    q[45:60, 1] = -3.0
+    q[60:75, 2] += 0.5                    # not integral
+    adj = knn_graph(base, 32, 31, seed=dim)
+    meta = dict(kind="l2", block_size=32, pq_size=512, bf_words=512, bf_nhash=4,
+                n_multiprobe=4, k=10, ef=128)
+    a = dict(base=base, queries=q, adj=adj)
+    g = song.KernelGraph(base.shape[0], dim, base, song.Params(pq_size=512), adj=adj)
+    g.upload_to_gpu()
+    assert g.u8_rows() == (dim + 15) // 16 * 16
+    g.close()
+    ids, tr = song_search(song, meta, a)
+    oids, otr = oracle_run(oracle, meta, a)
+    np.testing.assert_array_equal(ids, oids)
+    np.testing.assert_array_equal(tr.queries, otr)
+
+
+def test_no_byte_rows_outside_range(cuda, song):
+    base = np.full((50, 16), 256.0, np.float32)
+    g = song.KernelGraph(50, 16, base, song.Params(), adj=np.full((50, 32), -1, np.int32))
+    g.upload_to_gpu()
+    assert g.u8_rows() == 0
+    g.close()
