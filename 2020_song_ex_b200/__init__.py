@@ -161,6 +161,13 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_server_run_poisson.argtypes = [vp, vp, ci, vp, vp, vp, C.c_double, C.c_uint, vp, vp,
                                           C.POINTER(C.c_double)]
     L.song_server_destroy.argtypes = [vp]
+    L.song_search_device_seeded.argtypes = [vp, C.POINTER(_Opts), vp, ci, ci, ci, vp, ci, vp, vp,
+                                            vp, vp]
+    L.song_search_device_seeded.restype = C.c_int
+    L.song_index_set_entry_hubs.argtypes = [vp, vp, ci]
+    L.song_index_set_entry_hubs.restype = C.c_int
+    L.song_index_entry_candidates.argtypes = [vp, vp, ci, vp, vp, vp]
+    L.song_index_entry_candidates.restype = C.c_int
     L.song_index_u8_rows.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
     L.song_index_u8_rows.restype = C.c_int
     L.song_bithash_matrix.argtypes = [ci, ci, C.c_uint, vp]
@@ -472,6 +479,43 @@ def search_device_ex(g, opts: Optional[SearchOpts], d_queries, nq: int, k: int, 
     _check(load_library().song_search_device_ex(g._h, C.byref(o), ptr(d_queries), nq, k,
                                                 ef_search, ptr(d_ids), ptr(d_dists),
                                                 ptr(d_traces), st))
+
+
+ENTRY_K = 24  # entry candidates per query (the entry model's inputs)
+
+
+def set_entry_hubs(g: KernelGraph, hub_ids) -> None:
+    """Attach the hub set of the learned entry stage (node ids)."""
+    h = np.ascontiguousarray(np.asarray(hub_ids, np.int32).reshape(-1))
+    _check(load_library().song_index_set_entry_hubs(g._h, h.ctypes.data, int(h.size)))
+
+
+def entry_candidates(g: KernelGraph, d_queries, nq: int, d_ids, d_dists, stream=None) -> None:
+    """The entry stage alone: each query's 24 nearest hubs (device int32 /
+    float32 [nq, 24]), from the tensor-core kernel."""
+    st = None
+    if stream is not None:
+        st = int(getattr(stream, "cuda_stream", stream))
+    _check(load_library().song_index_entry_candidates(
+        g._h, int(d_queries.data_ptr()), nq, int(d_ids.data_ptr()), int(d_dists.data_ptr()), st))
+
+
+def search_device_seeded(g, opts: Optional[SearchOpts], d_queries, nq: int, k: int,
+                         ef_search: int, d_seeds, n_seeds: int, d_ids, d_dists=None,
+                         d_traces=None, stream=None) -> None:
+    """song_search_device_seeded: the extended search from per-query entry
+    points d_seeds [nq, n_seeds] (device int32) instead of p*n/N_MULTIPROBE."""
+    def ptr(x):
+        if x is None:
+            return None
+        return int(x.data_ptr()) if hasattr(x, "data_ptr") else int(x)
+    st = None
+    if stream is not None:
+        st = int(getattr(stream, "cuda_stream", stream))
+    o = (opts or SearchOpts())._c()
+    _check(load_library().song_search_device_seeded(g._h, C.byref(o), ptr(d_queries), nq, k,
+                                                    ef_search, ptr(d_seeds), n_seeds, ptr(d_ids),
+                                                    ptr(d_dists), ptr(d_traces), st))
 
 
 def gpu_search_ex(g, opts: Optional[SearchOpts], queries, nq: int, k: int,

@@ -11,6 +11,7 @@
 //    max(n_multiquery, 16384) and runs each chunk as ONE persistent launch
 //    (results do not depend on batching: queries are independent).
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 
 #include <algorithm>
 #include <atomic>
@@ -63,6 +64,18 @@ struct song_index {
     void* d_fp8 = nullptr;
     float* d_fp8_scale = nullptr;
     int fp8_ld = 0;
+    // hub set of the learned entry stage: BF16 tensor-core tiles of the hub
+    // rows, their squared norms and node ids (padded to whole tiles)
+    std::vector<int32_t> entry_hubs;
+    int entry_hpad = 0;
+    int32_t* d_entry_ids = nullptr;
+    __nv_bfloat16* d_entry_tiles = nullptr;
+    float* d_entry_norm = nullptr;
+    // per-query entry candidates of a launch (grown on demand)
+    int32_t* d_ecand = nullptr;
+    size_t ecand_cap = 0;
+    float* d_edist = nullptr;
+    size_t edist_cap = 0;
     // learned entry / stop models
     bool has_model = false;
     std::vector<int32_t> hubs;
@@ -142,6 +155,11 @@ void free_index(song_index* x) {
     cudaFree(x->d_tr);
     cudaFree(x->d_dist);
     cudaFree(x->d_u8);
+    cudaFree(x->d_entry_ids);
+    cudaFree(x->d_entry_tiles);
+    cudaFree(x->d_entry_norm);
+    cudaFree(x->d_ecand);
+    cudaFree(x->d_edist);
     cudaFree(x->d_bf16);
     cudaFree(x->d_fp8);
     cudaFree(x->d_fp8_scale);
@@ -222,6 +240,52 @@ cudaError_t grow(T** ptr, size_t* cap, size_t bytes) {
     cudaError_t e = cudaMalloc((void**)ptr, bytes);
     if (e == cudaSuccess) *cap = bytes;
     return e;
+}
+
+// Build the entry stage's tables for hub node ids `hubs` (device, stream-ordered).
+song_status attach_entry_hubs(song_index* x, const std::vector<int32_t>& hubs) {
+    if (x->kind != SONG_KIND_L2) return fail(SONG_ERR_UNSUPPORTED, "entry hubs apply to L2 indexes");
+    if (x->dim > song::kEntryMaxDim) return fail(SONG_ERR_UNSUPPORTED, "entry hubs need dim <= 288");
+    if (hubs.empty()) return fail(SONG_ERR_INVALID_ARG, "empty hub set");
+    for (int32_t h : hubs)
+        if (h < 0 || h >= x->n) return fail(SONG_ERR_INVALID_ARG, "hub id out of range");
+    const int tile = song::entry_tile_hubs();
+    const int hpad = ((int)hubs.size() + tile - 1) / tile * tile;
+    const int kp = song::entry_padded_dim(x->dim);
+    std::vector<int32_t> ids(hubs);
+    ids.resize(hpad, -1);
+    cudaFree(x->d_entry_ids);
+    cudaFree(x->d_entry_tiles);
+    cudaFree(x->d_entry_norm);
+    x->d_entry_ids = nullptr;
+    x->d_entry_tiles = nullptr;
+    x->d_entry_norm = nullptr;
+    x->entry_hpad = 0;
+    x->entry_hubs.clear();
+    cudaError_t e = cudaMalloc(&x->d_entry_ids, (size_t)hpad * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&x->d_entry_tiles, (size_t)hpad * kp * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&x->d_entry_norm, (size_t)hpad * 4);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(x->d_entry_ids, ids.data(), (size_t)hpad * 4, cudaMemcpyHostToDevice,
+                            x->stream);
+    if (e == cudaSuccess)
+        e = song::build_entry_tables((const float*)x->d_base, x->ld, x->dim, x->d_entry_ids, hpad,
+                                     x->d_entry_tiles, x->d_entry_norm, x->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "entry hub tables");
+    x->entry_hubs = hubs;
+    x->entry_hpad = hpad;
+    return SONG_OK;
+}
+
+// The entry stage for nq queries at d_q: ids/dists [nq x kEntryK].
+song_status run_entry(song_index* x, const void* d_q, int nq, int32_t* d_ids, float* d_d,
+                      cudaStream_t st) {
+    cudaError_t e = song::launch_entry((const float*)d_q, x->dim, nq, x->dim, x->d_entry_tiles,
+                                       x->d_entry_norm, x->d_entry_ids, x->entry_hpad, d_ids, d_d,
+                                       x->d_err, st);
+    if (e != cudaSuccess) return cuda_fail(e, "entry launch");
+    return SONG_OK;
 }
 
 int clamp_ef(int ef, int k, int pq_size) {  // kernalGraph.h:315-316
@@ -617,6 +681,44 @@ song_status song_search_device_ex(song_index* x, const song_search_opts* opts,
     song::SearchArgs a;
     if (song_status s = make_args(x, d_queries, nq, k, ef, d_ids, d_traces, &a, opts, d_dists)) return s;
     return launch(x, a, (cudaStream_t)stream);
+}
+
+song_status song_search_device_seeded(song_index* x, const song_search_opts* opts,
+                                      const void* d_queries, int nq, int k, int ef_search,
+                                      const int32_t* d_seeds, int n_seeds, int32_t* d_ids,
+                                      float* d_dists, song_query_trace* d_traces, void* stream) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (nq < 0 || k < 0) return fail(SONG_ERR_INVALID_ARG, "nq and k must be >= 0");
+    if (nq == 0) return SONG_OK;
+    if (d_queries == nullptr || d_seeds == nullptr || (k > 0 && d_ids == nullptr))
+        return fail(SONG_ERR_INVALID_ARG, "queries, seeds or ids is NULL");
+    if (n_seeds < 1 || n_seeds > 32) return fail(SONG_ERR_INVALID_ARG, "n_seeds must be 1..32");
+    const int ef = clamp_ef(ef_search, k, x->p.pq_size);
+    std::lock_guard<std::mutex> lock(x->mu);
+    song::SearchArgs a;
+    if (song_status s = make_args(x, d_queries, nq, k, ef, d_ids, d_traces, &a, opts, d_dists)) return s;
+    a.qseeds = d_seeds;
+    a.n_qseeds = n_seeds;
+    return launch(x, a, (cudaStream_t)stream);
+}
+
+song_status song_index_set_entry_hubs(song_index* x, const int32_t* hub_ids, int count) {
+    if (x == nullptr || hub_ids == nullptr || count < 1)
+        return fail(SONG_ERR_INVALID_ARG, "index or hub ids missing");
+    std::lock_guard<std::mutex> lock(x->mu);
+    return attach_entry_hubs(x, std::vector<int32_t>(hub_ids, hub_ids + count));
+}
+
+song_status song_index_entry_candidates(song_index* x, const float* d_queries, int nq,
+                                        int32_t* d_ids, float* d_dists, void* stream) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (nq < 0) return fail(SONG_ERR_INVALID_ARG, "nq must be >= 0");
+    if (nq == 0) return SONG_OK;
+    if (d_queries == nullptr || d_ids == nullptr || d_dists == nullptr)
+        return fail(SONG_ERR_INVALID_ARG, "queries, ids or dists is NULL");
+    std::lock_guard<std::mutex> lock(x->mu);
+    if (x->entry_hpad == 0) return fail(SONG_ERR_INVALID_ARG, "no entry hub set attached");
+    return run_entry(x, d_queries, nq, d_ids, d_dists, (cudaStream_t)stream);
 }
 
 song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,

@@ -1,0 +1,346 @@
+// song_entry.cu -- entry points of the learned search: the nearest hubs of
+// every query, on the tensor cores.
+//
+// A hub set of H nodes (a few thousand) is laid out once, at learn time, as
+// BF16 tiles of 128 hubs in the tensor cores' shared-memory operand layout.
+// One CTA serves 128 queries: it converts their rows to BF16 into shared
+// memory (operand A), then for each hub tile
+//   * a bulk copy (cp.async.bulk, completion on an mbarrier) brings the tile
+//     into shared memory (operand B), double buffered so that the next
+//     tile's copy overlaps this tile's work;
+//   * one thread issues K/16 tcgen05.mma (kind::f16, BF16 x BF16 -> FP32,
+//     M = 128, N = 128) into a 128-column TMEM accumulator and commits them
+//     to an mbarrier;
+//   * every thread reads its query's row of the accumulator (tcgen05.ld,
+//     lane = query) and keeps the kEntryK hubs of smallest |h|^2 - 2 q.h in
+//     registers (|q|^2 is the same for every hub of a query).
+// The output is, per query, those hubs' node ids nearest first (ties: lower
+// hub index first) and their squared distances |q|^2 + |h|^2 - 2 q.h.  For
+// integer vectors in [0, 255] with dim <= 128 every BF16 value, product sum
+// and key stays an exact FP32 integer below 2^24, so the distances are
+// exact; otherwise they carry BF16 rounding, which only matters for the
+// choice of entry points.
+//
+// Shared-memory operand layout (no swizzle, K-major): 8 x 16-byte core
+// matrices, one per 8 rows x 8 elements; core matrices adjacent along K are
+// 128 bytes apart (the descriptor's leading byte offset), groups of 8 rows
+// are (Kp / 8) * 128 bytes apart (its stride byte offset).
+//
+// Every wait is bounded: a barrier that does not complete within about two
+// seconds sets the error word, the CTA stops issuing work, and it still
+// frees its tensor memory before it returns.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+
+#include "song_kernels.cuh"
+
+namespace song {
+extern std::atomic<int64_t> g_launches;
+
+namespace {
+
+constexpr int kM = 128;           // queries per CTA (MMA M)
+constexpr int kN = 128;           // hubs per tile (MMA N), TMEM columns of the accumulator
+constexpr int kK = kEntryK;       // nearest hubs kept per query
+constexpr long long kWaitNs = 2000000000LL;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ long long now_ns() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for the mbarrier phase with parity `parity`; false after ~2 s.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    const long long t0 = now_ns();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (now_ns() - t0 > kWaitNs) return false;
+    }
+}
+
+// Shared-memory matrix descriptor (tcgen05): start, leading and stride byte
+// offsets in 16-byte units, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t start, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((start >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N = 128, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
+                            ((uint32_t)(kM >> 4) << 24);
+
+// Byte offset of element (r, k) of a K-major operand tile with Kp columns.
+__host__ __device__ __forceinline__ uint32_t tile_off(int r, int k, int kp) {
+    return (uint32_t)((r >> 3) * (kp >> 3) * 128 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+struct EntryArgs {
+    const float* queries;      // [nq x qld] FP32
+    int qld, nq, dim, kp;      // kp = dim rounded up to 16
+    const __nv_bfloat16* hub_tiles;  // [ntiles][kN x kp] in the operand layout
+    const float* hub_norm;     // [ntiles * kN], +inf for padding
+    const int32_t* hub_ids;    // [ntiles * kN], -1 for padding
+    int ntiles;
+    int32_t* out_ids;          // [nq x kK]
+    float* out_d;              // [nq x kK]
+    int* err;                  // set to 2 when a bounded wait gives up
+};
+
+__global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar_load[2];
+    __shared__ __align__(8) uint64_t bar_mma;
+    __shared__ uint32_t tslot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t a_bytes = (uint32_t)kM * a.kp * 2, b_bytes = (uint32_t)kN * a.kp * 2;
+    unsigned char* As = smem;
+    unsigned char* Bs[2] = {smem + a_bytes, smem + a_bytes + b_bytes};
+    const uint32_t sbo = (uint32_t)(a.kp >> 3) * 128;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_addr(&tslot)), "r"(kN) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_load[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_load[1])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_mma)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tslot;
+
+    // first hub tiles in flight while the queries are converted
+    auto issue_load = [&](int t, int buf) {
+        const uint32_t bar = smem_addr(&bar_load[buf]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     :: "r"(bar), "r"(b_bytes) : "memory");
+        const __nv_bfloat16* src = a.hub_tiles + (size_t)t * kN * a.kp;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+            :: "r"(smem_addr(Bs[buf])), "l"(src), "r"(b_bytes), "r"(bar) : "memory");
+    };
+    if (tid == 0) {
+        issue_load(0, 0);
+        if (a.ntiles > 1) issue_load(1, 1);
+    }
+
+    // operand A: this thread's query as BF16, and its FP32 squared norm
+    const int q = blockIdx.x * kM + tid;
+    float qn = 0.0f;
+    for (int k0 = 0; k0 < a.kp; k0 += 8) {
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int k = k0 + e;
+            const float x = (q < a.nq && k < a.dim) ? a.queries[(size_t)q * a.qld + k] : 0.0f;
+            qn = fmaf(x, x, qn);
+            v[e] = __float2bfloat16_rn(x);
+        }
+        *reinterpret_cast<uint4*>(As + tile_off(tid, k0, a.kp)) = *reinterpret_cast<const uint4*>(v);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
+    __syncthreads();
+
+    float kd[kK];
+    int ki[kK];
+#pragma unroll
+    for (int i = 0; i < kK; ++i) {
+        kd[i] = INFINITY;
+        ki[i] = -1;
+    }
+    bool ok = true;
+    for (int t = 0; t < a.ntiles; ++t) {
+        const int buf = t & 1;
+        // a wait that gives up in any thread ends the loop in every thread
+        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_load[buf]), (uint32_t)((t >> 1) & 1)));
+        if (!ok) break;
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs[buf]);
+            for (int s = 0; s < a.kp / 16; ++s) {
+                const uint64_t ad = umma_desc(a0 + (uint32_t)s * 256u, 128u, sbo);
+                const uint64_t bd = umma_desc(b0 + (uint32_t)s * 256u, 128u, sbo);
+                const uint32_t acc = s > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    :: "r"(tmem), "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc) : "memory");
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                :: "r"(smem_addr(&bar_mma)) : "memory");
+        }
+        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_mma), (uint32_t)(t & 1)));
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // the MMAs have read this buffer: refill it with tile t + 2
+        if (tid == 0 && t + 2 < a.ntiles) issue_load(t + 2, buf);
+        const float* hn = a.hub_norm + (size_t)t * kN;
+        const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < kN; c0 += 32) {
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+                "tcgen05.wait::ld.sync.aligned;"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                  "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                  "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
+                  "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                  "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+                  "=r"(r[30]), "=r"(r[31])
+                : "r"(row + (uint32_t)c0)
+                : "memory");
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const float d = fmaf(-2.0f, __uint_as_float(r[j]), __ldg(hn + c0 + j));
+                if (d < kd[kK - 1]) {  // sorted insertion; equal keys keep the earlier hub first
+                    const int idx = t * kN + c0 + j;
+#pragma unroll
+                    for (int i = kK - 1; i > 0; --i) {
+                        const bool shift = d < kd[i - 1];
+                        const bool here = !shift && d < kd[i];
+                        kd[i] = shift ? kd[i - 1] : (here ? d : kd[i]);
+                        ki[i] = shift ? ki[i - 1] : (here ? idx : ki[i]);
+                    }
+                    if (d < kd[0]) {
+                        kd[0] = d;
+                        ki[0] = idx;
+                    }
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();  // every warp has read the accumulator before the next MMA
+    }
+    if (!ok && tid == 0) atomicExch(a.err, 2);
+    if (q < a.nq) {
+        for (int i = 0; i < kK; ++i) {
+            const bool v = ok && ki[i] >= 0 && kd[i] < INFINITY;
+            a.out_ids[(size_t)q * kK + i] = v ? __ldg(a.hub_ids + ki[i]) : -1;
+            a.out_d[(size_t)q * kK + i] = v ? fmaxf(qn + kd[i], 0.0f) : INFINITY;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kN)
+                     : "memory");
+}
+
+// Hub tiles from FP32 base rows: hub i of the set is node ids[i] (-1 =
+// padding: zero row, norm +inf).  One thread per 8-element chunk.
+__global__ void make_hub_tiles(const float* __restrict__ base, int ld, int dim, int kp,
+                               const int32_t* __restrict__ ids, int hpad,
+                               __nv_bfloat16* __restrict__ tiles) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int chunks = kp / 8;
+    if (c >= (int64_t)hpad * chunks) return;
+    const int h = (int)(c / chunks), k0 = (int)(c % chunks) * 8;
+    const int id = ids[h];
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const int k = k0 + e;
+        v[e] = __float2bfloat16_rn((id >= 0 && k < dim) ? base[(size_t)id * ld + k] : 0.0f);
+    }
+    const int t = h / kN, r = h % kN;
+    unsigned char* dst = reinterpret_cast<unsigned char*>(tiles + (size_t)t * kN * kp) + tile_off(r, k0, kp);
+    *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
+}
+
+// Squared norms of the BF16 hub rows (the values the tensor cores multiply).
+__global__ void hub_norms(const __nv_bfloat16* __restrict__ tiles, const int32_t* __restrict__ ids,
+                          int hpad, int kp, float* __restrict__ norm) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= hpad) return;
+    if (ids[h] < 0) {
+        norm[h] = INFINITY;
+        return;
+    }
+    const int t = h / kN, r = h % kN;
+    const unsigned char* tile = reinterpret_cast<const unsigned char*>(tiles + (size_t)t * kN * kp);
+    float s = 0.0f;
+    for (int k = 0; k < kp; ++k) {
+        const float x = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(tile + tile_off(r, k, kp)));
+        s = fmaf(x, x, s);
+    }
+    norm[h] = s;
+}
+
+}  // namespace
+
+int entry_padded_dim(int dim) { return (dim + 15) / 16 * 16; }
+int entry_tile_hubs() { return kN; }
+
+cudaError_t build_entry_tables(const float* d_base, int ld, int dim, const int32_t* d_ids,
+                               int hpad, __nv_bfloat16* d_tiles, float* d_norm, cudaStream_t st) {
+    const int kp = entry_padded_dim(dim);
+    const int64_t work = (int64_t)hpad * (kp / 8);
+    make_hub_tiles<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(d_base, ld, dim, kp, d_ids, hpad,
+                                                                    d_tiles);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    hub_norms<<<(hpad + 127) / 128, 128, 0, st>>>(d_tiles, d_ids, hpad, kp, d_norm);
+    return cudaGetLastError();
+}
+
+size_t entry_smem_bytes(int dim) {
+    const size_t kp = (size_t)entry_padded_dim(dim);
+    return (size_t)kM * kp * 2 + 2 * (size_t)kN * kp * 2;
+}
+
+cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
+                         const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
+                         int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
+                         cudaStream_t st) {
+    if (nq <= 0) return cudaSuccess;
+    if (dim > kEntryMaxDim || hpad % kN != 0 || hpad <= 0) return cudaErrorInvalidValue;
+    EntryArgs a;
+    a.queries = d_queries;
+    a.qld = qld;
+    a.nq = nq;
+    a.dim = dim;
+    a.kp = entry_padded_dim(dim);
+    a.hub_tiles = d_tiles;
+    a.hub_norm = d_norm;
+    a.hub_ids = d_ids;
+    a.ntiles = hpad / kN;
+    a.out_ids = d_out_ids;
+    a.out_d = d_out_d;
+    a.err = d_err;
+    const size_t smem = entry_smem_bytes(dim);
+    cudaError_t e = cudaFuncSetAttribute(entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    entry_kernel<<<(unsigned)((nq + kM - 1) / kM), 128, smem, st>>>(a);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return cudaGetLastError();
+}
+
+}  // namespace song

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <cuda_fp16.h>
+#include <cuda_bf16.h>
 
 #include <vector>
 
@@ -30,6 +31,8 @@ struct SearchArgs {
     int bf_words;            // BF_WORDS
     int bf_nhash;            // BF_NHASH (1..4)
     int n_multiprobe;        // N_MULTIPROBE
+    const int32_t* qseeds;   // [nq x n_qseeds] entry points per query (-1 = none), or nullptr
+    int n_qseeds;            // 1..32
     int warp_smem;           // bytes of shared memory per warp (multiple of 16)
     int q_off, rows_off, cd_off, ci_off, rd_off, ri_off, bl_off;  // per-warp carve-up, bytes
     int tm_cols;             // TMEM columns one CTA allocates (set by launch_search)
@@ -69,6 +72,26 @@ constexpr int kHid = 64;
 // Packed FP16 / FP32 parameter layout: W1[kHid][kFeat] b1[kHid] W2[kHid][kHid] b2[kHid]
 // W3[out][kHid] b3[out].
 constexpr int mlp_param_count(int out) { return kHid * kFeat + kHid + kHid * kHid + kHid + out * kHid + out; }
+
+// Entry points of the learned search (song_entry.cu): every query's
+// kEntryK nearest hubs from a hub set laid out as BF16 tensor-core tiles.
+constexpr int kEntryK = kFeat;
+constexpr int kEntryMaxDim = 288;
+int entry_padded_dim(int dim);
+int entry_tile_hubs();
+size_t entry_smem_bytes(int dim);
+// Lay out hubs (node ids, -1 = padding; hpad a multiple of entry_tile_hubs())
+// of FP32 base rows as BF16 tiles [hpad x entry_padded_dim(dim)] and their
+// squared norms (+inf for padding).  Stream-ordered.
+cudaError_t build_entry_tables(const float* d_base, int ld, int dim, const int32_t* d_ids,
+                               int hpad, __nv_bfloat16* d_tiles, float* d_norm, cudaStream_t st);
+// out_ids / out_d [nq x kEntryK]: each query's nearest hubs (node ids, -1 if
+// none) and squared distances, nearest first.  err is set to 2 if a bounded
+// wait gives up.
+cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
+                         const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
+                         int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
+                         cudaStream_t st);
 
 // Padded element count of a compressed row (a whole number of 128-byte
 // lines per 8-lane group) and its byte stride.

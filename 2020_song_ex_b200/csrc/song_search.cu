@@ -1102,8 +1102,17 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     StopState ss;
     stop_init(ss, a.k);
     int seed_id = -1, n_seeds = a.n_multiprobe;
+    const bool given_seeds = a.qseeds != nullptr;  // caller-chosen entry points per query
+    if (given_seeds) {
+        n_seeds = a.n_qseeds;
+        seed_id = lane < n_seeds ? __ldg(a.qseeds + (int64_t)qid * a.n_qseeds + lane) : -1;
+        if (seed_id >= a.n) {  // never read out of range
+            atomicExch(a.err, 1);
+            seed_id = -1;
+        }
+    }
     if constexpr (LM > 0) {
-        if (a.n_hubs > 0) {
+        if (a.n_hubs > 0 && !given_seeds) {
             const int hub = lane < a.n_hubs ? __ldg(a.hubs + lane) : -1;
             const unsigned HN = __ballot_sync(FULL, hub >= 0);
             const float hd = distances(hub, HN);
@@ -1223,7 +1232,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             int nb = -1;
             if (j < limit) {
                 if (seeding) {
-                    nb = (LM > 0 && seed_id >= 0) ? seed_id
+                    nb = (given_seeds || (LM > 0 && seed_id >= 0)) ? seed_id
                                                   : (int)((unsigned long long)j * (unsigned long long)a.n /
                                                           (unsigned long long)a.n_multiprobe);
                 } else {

@@ -248,6 +248,19 @@ song_status song_search_device_ex(song_index* index, const song_search_opts* opt
                                   int32_t* d_ids, float* d_dists, song_query_trace* d_traces,
                                   void* stream);
 
+/*
+ * The extended search from caller-chosen entry points (no counterpart in the
+ * reference, whose entry points are always p*n/N_MULTIPROBE,
+ * kernalGraph.h:214-231): d_seeds [nq x n_seeds] (device int32, 1 <= n_seeds
+ * <= 32, -1 = no entry) replaces the N_MULTIPROBE seeds of each query; the
+ * rest is song_search_device_ex.  An id >= n is skipped and reported through
+ * the index's error word.
+ */
+song_status song_search_device_seeded(song_index* index, const song_search_opts* opts,
+                                      const void* d_queries, int nq, int k, int ef_search,
+                                      const int32_t* d_seeds, int n_seeds, int32_t* d_ids,
+                                      float* d_dists, song_query_trace* d_traces, void* stream);
+
 /* The extended search with host buffers (gpu_search-style, synchronous). */
 song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,
                                const float* queries, int nq, int k, int n_multiquery,
@@ -295,6 +308,21 @@ void song_learn_params_default(song_learn_params* p);
 song_status song_index_learn(song_index* index, const song_learn_params* params,
                              const float* d_train_queries, int nq, const int32_t* d_train_nn1,
                              song_learn_report* report);
+
+/*
+ * Hub set of the learned entry stage (no counterpart in the reference).
+ * song_index_set_entry_hubs attaches `count` hub node ids to an L2 index
+ * (dim <= 288): their rows are laid out once as BF16 tensor-core tiles.
+ * song_index_learn chooses and attaches a hub set itself.
+ * song_index_entry_candidates runs the entry stage alone: for each query
+ * (device FP32 [nq x dim]) the 24 nearest hubs by BF16 tensor-core distance,
+ * nearest first (ties: earlier hub first), as node ids (-1 when the set has
+ * fewer hubs) and squared distances (device [nq x 24] each); exact for
+ * integer vectors in [0, 255] with dim <= 128.  Asynchronous on `stream`.
+ */
+song_status song_index_set_entry_hubs(song_index* index, const int32_t* hub_ids, int count);
+song_status song_index_entry_candidates(song_index* index, const float* d_queries, int nq,
+                                        int32_t* d_ids, float* d_dists, void* stream);
 
 /* Flat FP32 copy of the attached models (*length floats; blob may be NULL to query). */
 song_status song_index_get_model(const song_index* index, float* blob, int capacity, int* length);
