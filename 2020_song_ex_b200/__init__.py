@@ -91,7 +91,7 @@ class _LearnParams(C.Structure):
     _fields_ = [("k", C.c_int), ("ef", C.c_int), ("ckpt_every", C.c_int),
                 ("min_expansions", C.c_int), ("max_ckpt", C.c_int), ("entry_steps", C.c_int),
                 ("stop_steps", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
-                ("seed", C.c_uint)]
+                ("seed", C.c_uint), ("entry_hubs", C.c_int)]
 
 
 class _LearnReport(C.Structure):
@@ -168,6 +168,10 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_index_set_entry_hubs.restype = C.c_int
     L.song_index_entry_candidates.argtypes = [vp, vp, ci, vp, vp, vp]
     L.song_index_entry_candidates.restype = C.c_int
+    L.song_graph_search.argtypes = [vp, vp, ci, ci, ci, vp, vp]
+    L.song_graph_search.restype = C.c_int
+    L.song_graph_search_device.argtypes = [vp, vp, ci, ci, ci, vp, vp, vp]
+    L.song_graph_search_device.restype = C.c_int
     L.song_index_u8_rows.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
     L.song_index_u8_rows.restype = C.c_int
     L.song_bithash_matrix.argtypes = [ci, ci, C.c_uint, vp]
@@ -481,6 +485,17 @@ def search_device_ex(g, opts: Optional[SearchOpts], d_queries, nq: int, k: int, 
                                                 ptr(d_traces), st))
 
 
+def graph_search(g: KernelGraph, queries, nq: int, k: int, ef_search: int = 0):
+    """Graph::search (graph.h:33-115) on the GPU: returns (ids [nq, k] worst-first
+    as the reference returns them, -1 padded; traces int32 [nq, 12])."""
+    q = np.ascontiguousarray(np.asarray(queries, np.float32).reshape(nq, -1))
+    ids = np.empty((nq, k), np.int32)
+    tr = np.zeros((nq, 12), np.int32)
+    _check(load_library().song_graph_search(g._h, q.ctypes.data, nq, k, ef_search,
+                                            ids.ctypes.data, tr.ctypes.data))
+    return ids, tr
+
+
 ENTRY_K = 24  # entry candidates per query (the entry model's inputs)
 
 
@@ -552,11 +567,12 @@ class LearnParams:
     batch: int = 4096
     lr: float = 2e-3
     seed: int = 2020
+    entry_hubs: int = 4096  # hub set of the tensor-core entry stage; 0 = 24 in-kernel hubs
 
     def _c(self) -> _LearnParams:
         return _LearnParams(self.k, self.ef, self.ckpt_every, self.min_expansions, self.max_ckpt,
                             self.entry_steps, self.stop_steps, self.batch, float(self.lr),
-                            int(self.seed))
+                            int(self.seed), int(self.entry_hubs))
 
 
 def learn(g: KernelGraph, d_train_queries, nq: int, d_train_nn1,

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -71,13 +72,18 @@ struct song_index {
     int32_t* d_entry_ids = nullptr;
     __nv_bfloat16* d_entry_tiles = nullptr;
     float* d_entry_norm = nullptr;
+    // exact visited bitmaps of the Graph::search mode, one per resident warp
+    uint32_t* d_visited = nullptr;
+    size_t visited_cap = 0;
     // per-query entry candidates of a launch (grown on demand)
     int32_t* d_ecand = nullptr;
     size_t ecand_cap = 0;
     float* d_edist = nullptr;
     size_t edist_cap = 0;
+    void* d_esplit = nullptr;  // split scratch of the entry stage (batches of <= 128 queries)
     // learned entry / stop models
     bool has_model = false;
+    bool model_staged = false;  // the entry model scores the entry stage's candidates
     std::vector<int32_t> hubs;
     std::vector<float> entry_p, stop_p;  // FP32 master parameters
     int32_t* d_hubs = nullptr;
@@ -159,6 +165,8 @@ void free_index(song_index* x) {
     cudaFree(x->d_entry_tiles);
     cudaFree(x->d_entry_norm);
     cudaFree(x->d_ecand);
+    cudaFree(x->d_visited);
+    cudaFree(x->d_esplit);
     cudaFree(x->d_edist);
     cudaFree(x->d_bf16);
     cudaFree(x->d_fp8);
@@ -281,9 +289,11 @@ song_status attach_entry_hubs(song_index* x, const std::vector<int32_t>& hubs) {
 // The entry stage for nq queries at d_q: ids/dists [nq x kEntryK].
 song_status run_entry(song_index* x, const void* d_q, int nq, int32_t* d_ids, float* d_d,
                       cudaStream_t st) {
+    if (x->d_esplit == nullptr)
+        SONG_CUDA(cudaMalloc(&x->d_esplit, song::entry_split_scratch_bytes()), "entry split scratch");
     cudaError_t e = song::launch_entry((const float*)d_q, x->dim, nq, x->dim, x->d_entry_tiles,
                                        x->d_entry_norm, x->d_entry_ids, x->entry_hpad, d_ids, d_d,
-                                       x->d_err, st);
+                                       x->d_err, st, x->d_esplit);
     if (e != cudaSuccess) return cuda_fail(e, "entry launch");
     return SONG_OK;
 }
@@ -348,7 +358,7 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
             return fail(SONG_ERR_UNSUPPORTED, "learned search: L2 indexes, queues up to 1024 slots");
         a->lm = 2;
         a->hubs = x->d_hubs;
-        a->n_hubs = (int)x->hubs.size();
+        a->n_hubs = x->model_staged ? 0 : (int)x->hubs.size();
         a->entry_w = x->d_entry_w;
         a->stop_w = x->d_stop_w;
         a->ckpt_every = x->ckpt_every;
@@ -373,6 +383,15 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
 }
 
 song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
+    if (a.lm == 2 && x->model_staged && a.qseeds == nullptr && a.ecand == nullptr && a.nq > 0) {
+        // learned search: the entry stage first, on the same stream
+        const size_t cells = (size_t)a.nq * song::kEntryK;
+        SONG_CUDA(grow(&x->d_ecand, &x->ecand_cap, cells * 4), "entry candidates alloc");
+        SONG_CUDA(grow(&x->d_edist, &x->edist_cap, cells * 4), "entry distances alloc");
+        if (song_status s = run_entry(x, a.queries, a.nq, x->d_ecand, x->d_edist, st)) return s;
+        a.ecand = x->d_ecand;
+        a.edist = x->d_edist;
+    }
     unsigned* ctr = x->d_counter + (x->counter_next++ % kCounterRing);
     a.counter = ctr;
     SONG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), st), "counter reset");
@@ -491,6 +510,13 @@ song_status server_args(song_index* x, const song_search_opts* opts, int max_k, 
 }
 
 int index_pq_size(const song_index* x) { return x ? x->p.pq_size : 0; }
+bool index_model_staged(const song_index* x) { return x && x->has_model && x->model_staged; }
+cudaError_t index_entry(song_index* x, const float* d_q, int qld, int nq, int32_t* d_ids,
+                        float* d_d, cudaStream_t st, void* split_scratch) {
+    return song::launch_entry(d_q, qld, nq, x->dim, x->d_entry_tiles, x->d_entry_norm,
+                              x->d_entry_ids, x->entry_hpad, d_ids, d_d, x->d_err, st,
+                              split_scratch);
+}
 int index_dim(const song_index* x) { return x ? x->dim : 0; }
 bool index_has_model(const song_index* x) { return x && x->has_model; }
 
@@ -702,6 +728,29 @@ song_status song_search_device_seeded(song_index* x, const song_search_opts* opt
     return launch(x, a, (cudaStream_t)stream);
 }
 
+// Graph::search on the GPU (see song_graphsearch.cu); ef_search raised to k
+// as graph.h:36 does.  Stream-ordered.
+song_status graph_search_launch(song_index* x, const float* d_q, int nq, int k, int ef_search,
+                                int32_t* d_ids, song_query_trace* d_tr, cudaStream_t st) {
+    if (x->kind != SONG_KIND_L2) return fail(SONG_ERR_UNSUPPORTED, "Graph::search is the L2 search");
+    const int ef = ef_search < k ? k : ef_search;
+    if (ef < 1 || ef > 1024) return fail(SONG_ERR_UNSUPPORTED, "Graph::search mode: ef must be 1..1024");
+    if (ef < x->p.n_multiprobe)
+        return fail(SONG_ERR_UNSUPPORTED, "Graph::search mode: ef must be >= N_MULTIPROBE");
+    const int64_t warps = song::graph_search_resident_warps(x->dim, ef, x->num_sms, x->device);
+    if (warps < 4) return fail(SONG_ERR_UNSUPPORTED, "Graph::search mode: per-query state does not fit");
+    const int64_t vwords = (x->n + 31) / 32;
+    SONG_CUDA(grow(&x->d_visited, &x->visited_cap, (size_t)warps * vwords * 4), "visited bitmaps");
+    unsigned* ctr = x->d_counter + (x->counter_next++ % kCounterRing);
+    SONG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), st), "counter reset");
+    cudaError_t e = song::launch_graph_search((const float*)x->d_base, x->ld, x->dim, x->d_adj,
+                                              x->p.block_size, x->n, d_q, nq, k, ef,
+                                              x->p.n_multiprobe, d_ids, d_tr, ctr, x->d_err,
+                                              x->d_visited, warps, x->num_sms, st);
+    if (e != cudaSuccess) return cuda_fail(e, "Graph::search launch");
+    return SONG_OK;
+}
+
 song_status song_index_set_entry_hubs(song_index* x, const int32_t* hub_ids, int count) {
     if (x == nullptr || hub_ids == nullptr || count < 1)
         return fail(SONG_ERR_INVALID_ARG, "index or hub ids missing");
@@ -719,6 +768,51 @@ song_status song_index_entry_candidates(song_index* x, const float* d_queries, i
     std::lock_guard<std::mutex> lock(x->mu);
     if (x->entry_hpad == 0) return fail(SONG_ERR_INVALID_ARG, "no entry hub set attached");
     return run_entry(x, d_queries, nq, d_ids, d_dists, (cudaStream_t)stream);
+}
+
+song_status song_graph_search_device(song_index* x, const float* d_queries, int nq, int k,
+                                     int ef_search, int32_t* d_ids, song_query_trace* d_traces,
+                                     void* stream) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (nq < 0 || k < 1) return fail(SONG_ERR_INVALID_ARG, "nq must be >= 0 and k >= 1");
+    if (nq == 0) return SONG_OK;
+    if (d_queries == nullptr || d_ids == nullptr) return fail(SONG_ERR_INVALID_ARG, "queries or ids is NULL");
+    std::lock_guard<std::mutex> lock(x->mu);
+    return graph_search_launch(x, d_queries, nq, k, ef_search, d_ids, d_traces, (cudaStream_t)stream);
+}
+
+song_status song_graph_search(song_index* x, const float* queries, int nq, int k, int ef_search,
+                              int32_t* ids, song_query_trace* traces) {
+    if (x == nullptr) return fail(SONG_ERR_INVALID_ARG, "index is NULL");
+    if (nq < 0 || k < 1) return fail(SONG_ERR_INVALID_ARG, "nq must be >= 0 and k >= 1");
+    if (nq == 0) return SONG_OK;
+    if (queries == nullptr || ids == nullptr) return fail(SONG_ERR_INVALID_ARG, "queries or ids is NULL");
+    std::lock_guard<std::mutex> lock(x->mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != x->device) SONG_CUDA(cudaSetDevice(x->device), "cudaSetDevice");
+    cudaStream_t st = x->stream;
+    SONG_CUDA(grow(&x->d_q, &x->q_cap, (size_t)nq * x->dim * 4), "query alloc");
+    SONG_CUDA(grow(&x->d_ids, &x->ids_cap, (size_t)nq * k * 4), "ids alloc");
+    if (traces) SONG_CUDA(grow(&x->d_tr, &x->tr_cap, (size_t)nq * sizeof(song_query_trace)), "trace alloc");
+    SONG_CUDA(cudaMemsetAsync(x->d_err, 0, 4, st), "error reset");
+    SONG_CUDA(cudaMemcpyAsync(x->d_q, queries, (size_t)nq * x->dim * 4, cudaMemcpyHostToDevice, st),
+              "query copy");
+    if (song_status s = graph_search_launch(x, (const float*)x->d_q, nq, k, ef_search, x->d_ids,
+                                            traces ? x->d_tr : nullptr, st))
+        return s;
+    SONG_CUDA(cudaMemcpyAsync(ids, x->d_ids, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st), "ids copy");
+    if (traces)
+        SONG_CUDA(cudaMemcpyAsync(traces, x->d_tr, (size_t)nq * sizeof(song_query_trace),
+                                  cudaMemcpyDeviceToHost, st), "trace copy");
+    int err = 0;
+    SONG_CUDA(cudaMemcpyAsync(&err, x->d_err, 4, cudaMemcpyDeviceToHost, st), "error word");
+    SONG_CUDA(cudaStreamSynchronize(st), "Graph::search");
+    if (err == 3)
+        return fail(SONG_ERR_UNSUPPORTED, "Graph::search mode: more distance ties at the top-ef "
+                                          "maximum than the frontier holds");
+    if (err != 0) return fail(SONG_ERR_CUDA, "Graph::search: the kernel reported an error");
+    return SONG_OK;
 }
 
 song_status song_gpu_search_ex(song_index* index, const song_search_opts* opts,
@@ -740,6 +834,7 @@ void song_learn_params_default(song_learn_params* p) {
     p->stop_steps = 3000;
     p->batch = 4096;
     p->lr = 2e-3f;
+    p->entry_hubs = 4096;
     p->seed = 2020;
 }
 
@@ -779,6 +874,39 @@ song_status song_index_learn(song_index* x, const song_learn_params* lp,
     a.counter = x->d_counter;
     a.ckpt_every = lp->ckpt_every;
     a.min_expansions = lp->min_expansions;
+    // The entry stage: a hub set of entry_hubs nodes (a seeded sample) laid out
+    // for the tensor cores; the training queries' candidates feed the traces.
+    const bool staged = lp->entry_hubs > 0 && x->dim <= song::kEntryMaxDim;
+    int32_t* d_tc = nullptr;
+    float* d_td = nullptr;
+    if (staged) {
+        const int64_t H = std::min<int64_t>(lp->entry_hubs, x->n);
+        std::vector<int32_t> perm((size_t)x->n);
+        for (int64_t i = 0; i < x->n; ++i) perm[(size_t)i] = (int32_t)i;
+        std::mt19937_64 rng(lp->seed * 0x9E3779B97F4A7C15ull + 17u);
+        for (int64_t i = 0; i < H; ++i) {  // partial Fisher-Yates
+            std::uniform_int_distribution<int64_t> pick(i, x->n - 1);
+            std::swap(perm[(size_t)i], perm[(size_t)pick(rng)]);
+        }
+        perm.resize((size_t)H);
+        std::sort(perm.begin(), perm.end());
+        song_status s3 = attach_entry_hubs(x, perm);
+        cudaError_t e3 = cudaSuccess;
+        if (s3 == SONG_OK) {
+            e3 = cudaMalloc(&d_tc, (size_t)nq * song::kEntryK * 4);
+            if (e3 == cudaSuccess) e3 = cudaMalloc(&d_td, (size_t)nq * song::kEntryK * 4);
+            if (e3 != cudaSuccess) s3 = cuda_fail(e3, "entry candidates alloc");
+        }
+        if (s3 == SONG_OK) s3 = run_entry(x, d_train_queries, nq, d_tc, d_td, x->stream);
+        if (s3 != SONG_OK) {
+            cudaFree(d_ids);
+            cudaFree(d_tc);
+            cudaFree(d_td);
+            return s3;
+        }
+        a.ecand = d_tc;
+        a.edist = d_td;
+    }
     song::LearnInputs in{};
     in.args = a;
     in.base = x->d_base;
@@ -798,8 +926,11 @@ song_status song_index_learn(song_index* x, const song_learn_params* lp,
     song::LearnOutputs out;
     cudaError_t e = song::learn_models(in, &out);
     cudaFree(d_ids);
+    cudaFree(d_tc);
+    cudaFree(d_td);
     if (e != cudaSuccess) return cuda_fail(e, "learn");
     x->hubs = out.hubs;
+    x->model_staged = staged;
     x->entry_p = out.entry;
     x->stop_p = out.stop;
     x->ckpt_every = lp->ckpt_every;
@@ -807,7 +938,7 @@ song_status song_index_learn(song_index* x, const song_learn_params* lp,
     x->model_k = lp->k;
     if (song_status s2 = attach_model(x)) return s2;
     if (report) {
-        report->n_hubs = (int)out.hubs.size();
+        report->n_hubs = staged ? (int)x->entry_hubs.size() : (int)out.hubs.size();
         report->stop_samples = out.stop_samples;
         report->entry_loss_first = out.entry_loss_first;
         report->entry_loss_last = out.entry_loss_last;
@@ -825,15 +956,22 @@ song_status song_index_get_model(const song_index* x, float* blob, int capacity,
     if (!x->has_model) return fail(SONG_ERR_INVALID_ARG, "no learned model attached");
     std::vector<float> v;
     auto put_u = [&](uint32_t u) { float f; std::memcpy(&f, &u, 4); v.push_back(f); };
+    // version 1: [magic 1 n_hubs ckpt min_exp k n_entry n_stop] hubs entry stop
+    // version 2 (entry stage): [magic 2 n_out ckpt min_exp k n_entry n_stop n_set] set entry stop
     put_u(kModelMagic);
-    put_u(1);
-    put_u((uint32_t)x->hubs.size());
+    put_u(x->model_staged ? 2u : 1u);
+    put_u(x->model_staged ? (uint32_t)song::kEntryK : (uint32_t)x->hubs.size());
     put_u((uint32_t)x->ckpt_every);
     put_u((uint32_t)x->min_expansions);
     put_u((uint32_t)x->model_k);
     put_u((uint32_t)x->entry_p.size());
     put_u((uint32_t)x->stop_p.size());
-    for (int32_t h : x->hubs) put_u((uint32_t)h);
+    if (x->model_staged) {
+        put_u((uint32_t)x->entry_hubs.size());
+        for (int32_t h : x->entry_hubs) put_u((uint32_t)h);
+    } else {
+        for (int32_t h : x->hubs) put_u((uint32_t)h);
+    }
     v.insert(v.end(), x->entry_p.begin(), x->entry_p.end());
     v.insert(v.end(), x->stop_p.begin(), x->stop_p.end());
     *length = (int)v.size();
@@ -847,22 +985,33 @@ song_status song_index_get_model(const song_index* x, float* blob, int capacity,
 song_status song_index_set_model(song_index* x, const float* blob, int length) {
     if (x == nullptr || blob == nullptr || length < 8) return fail(SONG_ERR_INVALID_ARG, "bad model blob");
     auto get_u = [&](int i) { uint32_t u; std::memcpy(&u, blob + i, 4); return u; };
-    if (get_u(0) != kModelMagic || get_u(1) != 1) return fail(SONG_ERR_INVALID_ARG, "not a model blob");
+    const uint32_t ver = get_u(1);
+    if (get_u(0) != kModelMagic || (ver != 1 && ver != 2)) return fail(SONG_ERR_INVALID_ARG, "not a model blob");
     const int nh = (int)get_u(2), ne = (int)get_u(6), ns = (int)get_u(7);
-    if (nh < 1 || nh > song::kFeat || ne != song::mlp_param_count(nh) ||
-        ns != song::mlp_param_count(1) || length != 8 + nh + ne + ns)
+    const int hdr = ver == 2 ? 9 : 8;
+    const int nset = ver == 2 ? (length >= 9 ? (int)get_u(8) : -1) : nh;
+    if (nh < 1 || nh > song::kFeat || (ver == 2 && nh != song::kEntryK) || nset < 1 ||
+        ne != song::mlp_param_count(nh) || ns != song::mlp_param_count(1) ||
+        length != hdr + nset + ne + ns)
         return fail(SONG_ERR_INVALID_ARG, "model blob sizes do not match");
     std::lock_guard<std::mutex> lock(x->mu);
-    x->hubs.resize(nh);
-    for (int i = 0; i < nh; ++i) {
-        x->hubs[i] = (int32_t)get_u(8 + i);
-        if (x->hubs[i] < 0 || x->hubs[i] >= x->n) return fail(SONG_ERR_INVALID_ARG, "hub id out of range");
+    std::vector<int32_t> ids((size_t)nset);
+    for (int i = 0; i < nset; ++i) {
+        ids[(size_t)i] = (int32_t)get_u(hdr + i);
+        if (ids[(size_t)i] < 0 || ids[(size_t)i] >= x->n) return fail(SONG_ERR_INVALID_ARG, "hub id out of range");
     }
+    if (ver == 2) {
+        if (song_status s2 = attach_entry_hubs(x, ids)) return s2;
+        x->hubs.clear();
+    } else {
+        x->hubs = ids;
+    }
+    x->model_staged = ver == 2;
     x->ckpt_every = (int)get_u(3);
     x->min_expansions = (int)get_u(4);
     x->model_k = (int)get_u(5);
-    x->entry_p.assign(blob + 8 + nh, blob + 8 + nh + ne);
-    x->stop_p.assign(blob + 8 + nh + ne, blob + 8 + nh + ne + ns);
+    x->entry_p.assign(blob + hdr + nset, blob + hdr + nset + ne);
+    x->stop_p.assign(blob + hdr + nset + ne, blob + hdr + nset + ne + ns);
     return attach_model(x);
 }
 

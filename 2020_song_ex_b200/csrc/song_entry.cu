@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cstdint>
 
 #include "song_kernels.cuh"
@@ -99,8 +100,11 @@ struct EntryArgs {
     const float* hub_norm;     // [ntiles * kN], +inf for padding
     const int32_t* hub_ids;    // [ntiles * kN], -1 for padding
     int ntiles;
+    int tiles_per_split;       // blockIdx.y covers tiles [y * tps, (y + 1) * tps)
     int32_t* out_ids;          // [nq x kK]
     float* out_d;              // [nq x kK]
+    float* part_key;           // splits > 1: [splits x nq x kK] keys |h|^2 - 2 q.h
+    int32_t* part_idx;         // splits > 1: [splits x nq x kK] hub indices (-1 = none)
     int* err;                  // set to 2 when a bounded wait gives up
 };
 
@@ -131,6 +135,8 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tslot;
 
+    const int t_begin = blockIdx.y * a.tiles_per_split;
+    const int t_end = min(a.ntiles, t_begin + a.tiles_per_split);
     // first hub tiles in flight while the queries are converted
     auto issue_load = [&](int t, int buf) {
         const uint32_t bar = smem_addr(&bar_load[buf]);
@@ -142,8 +148,8 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
             :: "r"(smem_addr(Bs[buf])), "l"(src), "r"(b_bytes), "r"(bar) : "memory");
     };
     if (tid == 0) {
-        issue_load(0, 0);
-        if (a.ntiles > 1) issue_load(1, 1);
+        if (t_begin < t_end) issue_load(t_begin, 0);
+        if (t_begin + 1 < t_end) issue_load(t_begin + 1, 1);
     }
 
     // operand A: this thread's query as BF16, and its FP32 squared norm
@@ -171,10 +177,11 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
         ki[i] = -1;
     }
     bool ok = true;
-    for (int t = 0; t < a.ntiles; ++t) {
-        const int buf = t & 1;
+    for (int t = t_begin; t < t_end; ++t) {
+        const int u = t - t_begin;  // this CTA's u-th tile: buffer u % 2, its (u / 2)-th use
+        const int buf = u & 1;
         // a wait that gives up in any thread ends the loop in every thread
-        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_load[buf]), (uint32_t)((t >> 1) & 1)));
+        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_load[buf]), (uint32_t)((u >> 1) & 1)));
         if (!ok) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -193,11 +200,11 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                 :: "r"(smem_addr(&bar_mma)) : "memory");
         }
-        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_mma), (uint32_t)(t & 1)));
+        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_mma), (uint32_t)(u & 1)));
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // the MMAs have read this buffer: refill it with tile t + 2
-        if (tid == 0 && t + 2 < a.ntiles) issue_load(t + 2, buf);
+        if (tid == 0 && t + 2 < t_end) issue_load(t + 2, buf);
         const float* hn = a.hub_norm + (size_t)t * kN;
         const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
         for (int c0 = 0; c0 < kN; c0 += 32) {
@@ -239,10 +246,19 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     }
     if (!ok && tid == 0) atomicExch(a.err, 2);
     if (q < a.nq) {
-        for (int i = 0; i < kK; ++i) {
-            const bool v = ok && ki[i] >= 0 && kd[i] < INFINITY;
-            a.out_ids[(size_t)q * kK + i] = v ? __ldg(a.hub_ids + ki[i]) : -1;
-            a.out_d[(size_t)q * kK + i] = v ? fmaxf(qn + kd[i], 0.0f) : INFINITY;
+        if (gridDim.y > 1) {  // partial list of this split, merged by entry_merge
+            const size_t o = ((size_t)blockIdx.y * a.nq + q) * kK;
+            for (int i = 0; i < kK; ++i) {
+                const bool v = ok && ki[i] >= 0 && kd[i] < INFINITY;
+                a.part_key[o + i] = v ? kd[i] : INFINITY;
+                a.part_idx[o + i] = v ? ki[i] : -1;
+            }
+        } else {
+            for (int i = 0; i < kK; ++i) {
+                const bool v = ok && ki[i] >= 0 && kd[i] < INFINITY;
+                a.out_ids[(size_t)q * kK + i] = v ? __ldg(a.hub_ids + ki[i]) : -1;
+                a.out_d[(size_t)q * kK + i] = v ? fmaxf(qn + kd[i], 0.0f) : INFINITY;
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -251,6 +267,59 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kN)
                      : "memory");
+}
+
+// Merge of the splits' partial lists: one warp per query keeps the kK
+// smallest (key, hub index) -- the order the unsplit kernel keeps -- and
+// writes node ids and squared distances (|q|^2 from the FP32 query, as the
+// unsplit kernel adds it).
+__global__ void entry_merge(const float* __restrict__ part_key, const int32_t* __restrict__ part_idx,
+                            int splits, int nq, const float* __restrict__ queries, int qld, int dim,
+                            const int32_t* __restrict__ hub_ids, int32_t* __restrict__ out_ids,
+                            float* __restrict__ out_d) {
+    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= nq) return;
+    float qn = 0.0f;
+    if (lane == 0)
+        for (int k = 0; k < dim; ++k) {
+            const float x = queries[(size_t)q * qld + k];
+            qn = fmaf(x, x, qn);
+        }
+    qn = __shfl_sync(0xffffffffu, qn, 0);
+    const int total = splits * kK;
+    for (int i = 0; i < kK; ++i) {  // i-th smallest (key, index) over all splits
+        float bk = INFINITY;
+        int bi = INT_MAX, bs = -1;
+        for (int c = lane; c < total; c += 32) {
+            const size_t o = ((size_t)(c / kK) * nq + q) * kK + (c % kK);
+            const int idx = part_idx[o];
+            const float key = part_key[o];
+            if (idx >= 0 && (key < bk || (key == bk && idx < bi))) {
+                bk = key;
+                bi = idx;
+                bs = (int)o;
+            }
+        }
+#pragma unroll
+        for (int w = 16; w >= 1; w >>= 1) {
+            const float ok2 = __shfl_xor_sync(0xffffffffu, bk, w);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, w);
+            const int os = __shfl_xor_sync(0xffffffffu, bs, w);
+            if (os >= 0 && (bs < 0 || ok2 < bk || (ok2 == bk && oi < bi))) {
+                bk = ok2;
+                bi = oi;
+                bs = os;
+            }
+        }
+        if (lane == 0) {
+            out_ids[(size_t)q * kK + i] = bs >= 0 ? __ldg(hub_ids + bi) : -1;
+            out_d[(size_t)q * kK + i] = bs >= 0 ? fmaxf(qn + bk, 0.0f) : INFINITY;
+        }
+        __syncwarp();
+        if (lane == 0 && bs >= 0) const_cast<int32_t*>(part_idx)[bs] = -1;  // taken
+        __syncwarp();
+    }
 }
 
 // Hub tiles from FP32 base rows: hub i of the set is node ids[i] (-1 =
@@ -315,10 +384,12 @@ size_t entry_smem_bytes(int dim) {
     return (size_t)kM * kp * 2 + 2 * (size_t)kN * kp * 2;
 }
 
+size_t entry_split_scratch_bytes() { return (size_t)kEntrySplits * kM * kK * 8; }
+
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
-                         cudaStream_t st) {
+                         cudaStream_t st, void* split_scratch) {
     if (nq <= 0) return cudaSuccess;
     if (dim > kEntryMaxDim || hpad % kN != 0 || hpad <= 0) return cudaErrorInvalidValue;
     EntryArgs a;
@@ -333,12 +404,27 @@ cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
     a.ntiles = hpad / kN;
     a.out_ids = d_out_ids;
     a.out_d = d_out_d;
+    // A single tile of queries (serving batches) spreads its hub tiles over up
+    // to kEntrySplits CTAs, merged afterwards; larger batches use one CTA per
+    // 128 queries over all tiles.
+    int splits = 1;
+    if (nq <= kM && split_scratch != nullptr) splits = std::min(kEntrySplits, a.ntiles);
+    a.tiles_per_split = (a.ntiles + splits - 1) / splits;
+    splits = (a.ntiles + a.tiles_per_split - 1) / a.tiles_per_split;
+    a.part_key = static_cast<float*>(split_scratch);
+    a.part_idx = reinterpret_cast<int32_t*>(static_cast<char*>(split_scratch) +
+                                            (size_t)kEntrySplits * kM * kK * 4);
     a.err = d_err;
     const size_t smem = entry_smem_bytes(dim);
     cudaError_t e = cudaFuncSetAttribute(entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    entry_kernel<<<(unsigned)((nq + kM - 1) / kM), 128, smem, st>>>(a);
+    entry_kernel<<<dim3((unsigned)((nq + kM - 1) / kM), (unsigned)splits), 128, smem, st>>>(a);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || splits == 1) return e;
+    entry_merge<<<(nq + 3) / 4, 128, 0, st>>>(a.part_key, a.part_idx, splits, nq, d_queries, qld,
+                                              dim, d_ids, d_out_ids, d_out_d);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return cudaGetLastError();
 }

@@ -51,6 +51,8 @@ struct SearchArgs {
     float* out_dist;         // [nq x k] distance of each output id (nullable)
     // learned entry / stop (lm: 0 off, 1 collect traces of the full search, 2 infer)
     int lm;
+    const int32_t* ecand;    // [nq x kEntryK] entry-stage candidates (hub node ids, -1 = none), or nullptr
+    const float* edist;      // [nq x kEntryK] their squared distances
     const int32_t* hubs;     // [n_hubs] entry hub node ids (n_hubs <= kFeat)
     int n_hubs;
     const __half* entry_w;   // packed entry MLP (kFeat -> kHid -> kHid -> n_hubs), nullable
@@ -88,10 +90,24 @@ cudaError_t build_entry_tables(const float* d_base, int ld, int dim, const int32
 // out_ids / out_d [nq x kEntryK]: each query's nearest hubs (node ids, -1 if
 // none) and squared distances, nearest first.  err is set to 2 if a bounded
 // wait gives up.
+// split_scratch (entry_split_scratch_bytes(), nullable): lets batches of up
+// to 128 queries spread the hub tiles over several CTAs (serving).
+constexpr int kEntrySplits = 16;
+size_t entry_split_scratch_bytes();
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
-                         cudaStream_t st);
+                         cudaStream_t st, void* split_scratch = nullptr);
+
+// Graph::search (graph.h:33-115) bit for bit (song_graphsearch.cu).
+int graph_search_frontier_cap(int ef);
+size_t graph_search_warp_smem(int dim, int ef);
+int64_t graph_search_resident_warps(int dim, int ef, int num_sms, int dev);
+cudaError_t launch_graph_search(const float* d_base, int ld, int dim, const int32_t* d_adj, int bs,
+                                int64_t n, const float* d_queries, int nq, int k, int ef, int nmp,
+                                int32_t* d_out, song_query_trace* d_trace, unsigned* d_counter,
+                                int* d_err, uint32_t* d_visited, int64_t visited_slots,
+                                int num_sms, cudaStream_t st);
 
 // Padded element count of a compressed row (a whole number of 128-byte
 // lines per 8-lane group) and its byte stride.
@@ -158,10 +174,15 @@ struct ServeArgs {
     song_query_trace* res_trace;  // mapped host [slots]
     long long* res_done;        // mapped host [slots]: ticket completed in the slot
     long long* last_claim;      // device: %globaltimer (ns) of the latest claim
+    const int32_t* scand;       // device [slots x kEntryK]: entry-stage candidates per slot, or nullptr
+    const float* sdist;         // device [slots x kEntryK]: their squared distances
     long long idle_ns;          // a warp leaves once no request was claimed for this long
     int max_idle_polls, sleep_ns;  // hard bound on consecutive empty polls; poll backoff cap
 };
-cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStream_t st, int* warps_out);
+// reserve_sms > 0: one CTA per SM on num_sms - reserve_sms SMs, leaving the
+// rest to the entry stage (a learned model with a hub set).
+cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, int reserve_sms,
+                         cudaStream_t st, int* warps_out);
 
 // Training of the learned entry / stop models (song_learn.cu).
 struct LearnInputs {
@@ -194,6 +215,12 @@ song_status server_args(song_index* x, const song_search_opts* opts, int max_k, 
 int index_pq_size(const song_index* x);
 int index_dim(const song_index* x);
 bool index_has_model(const song_index* x);
+// The learned model scores the entry stage's candidates (song_index_learn
+// with entry_hubs > 0); index_entry runs that stage on nq queries that are
+// qld floats apart.
+bool index_model_staged(const song_index* x);
+cudaError_t index_entry(song_index* x, const float* d_q, int qld, int nq, int32_t* d_ids,
+                        float* d_d, cudaStream_t st, void* split_scratch = nullptr);
 
 // Records a failure message for song_last_error() on the calling thread.
 song_status set_error(song_status status, const char* message);

@@ -227,6 +227,35 @@ __global__ void entry_labels(const float* __restrict__ base, int ld, int dim,
     if (lane == 0) Y[q] = (float)arg;
 }
 
+// Entry labels when the entry stage supplies each query's kEntryK candidate
+// hubs: the candidate closest to the query's exact nearest neighbour (first
+// on ties; missing candidates never win).  One warp per query, lane j =
+// candidate j.
+__global__ void entry_labels_staged(const float* __restrict__ base, int ld, int dim,
+                                    const int32_t* __restrict__ cand,
+                                    const int32_t* __restrict__ nn1, int nq,
+                                    float* __restrict__ Y) {
+    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= nq) return;
+    const int c = lane < kEntryK ? cand[(size_t)q * kEntryK + lane] : -1;
+    float s = INFINITY;
+    if (c >= 0) {
+        const float* a = base + (size_t)nn1[q] * ld;
+        const float* b = base + (size_t)c * ld;
+        s = 0.0f;
+        for (int i = 0; i < dim; ++i) {
+            const float t = a[i] - b[i];
+            s = fmaf(t, t, s);
+        }
+    }
+    float best = s;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, w));
+    const unsigned win = __ballot_sync(0xffffffffu, c >= 0 && s == best);
+    if (lane == 0) Y[q] = win ? (float)(__ffs(win) - 1) : 0.0f;
+}
+
 template <typename T>
 cudaError_t dalloc(T** p, size_t count) {
     return cudaMalloc((void**)p, std::max<size_t>(1, count) * sizeof(T));
@@ -378,10 +407,15 @@ cudaError_t learn_models(const LearnInputs& in, LearnOutputs* out) {
     cudaStream_t st = in.stream;
     cudaError_t e = cudaSuccess;
     const int nq = in.nq, maxc = in.max_ckpt;
-    // 1) hubs
-    out->hubs = pick_hubs((const float*)in.base, in.n, in.dim, in.ld, kFeat, &e);
-    if (e != cudaSuccess) return e;
-    const int H = (int)out->hubs.size();
+    // 1) hubs: with the entry stage (args.ecand set) the entry model scores each
+    // query's kEntryK candidates; otherwise kFeat farthest-point hubs are scored
+    // inside the search kernel
+    const bool staged = in.args.ecand != nullptr;
+    if (!staged) {
+        out->hubs = pick_hubs((const float*)in.base, in.n, in.dim, in.ld, kFeat, &e);
+        if (e != cudaSuccess) return e;
+    }
+    const int H = staged ? kEntryK : (int)out->hubs.size();
     int32_t* d_hubs = nullptr;
     float *efeat = nullptr, *elab = nullptr, *tfeat = nullptr, *tkth = nullptr, *tfin = nullptr;
     int* tcnt = nullptr;
@@ -399,12 +433,12 @@ cudaError_t learn_models(const LearnInputs& in, LearnOutputs* out) {
         cleanup();
         return e;
     }
-    cudaMemcpyAsync(d_hubs, out->hubs.data(), H * 4, cudaMemcpyHostToDevice, st);
-    // 2) pass 1 (plain method): entry features
+    if (!staged) cudaMemcpyAsync(d_hubs, out->hubs.data(), H * 4, cudaMemcpyHostToDevice, st);
+    // 2) pass 1 (plain method from the nearest candidates when staged): entry features
     SearchArgs a = in.args;
     a.lm = 1;
     a.hubs = d_hubs;
-    a.n_hubs = H;
+    a.n_hubs = staged ? 0 : H;
     a.entry_w = nullptr;
     a.stop_w = nullptr;
     a.tr_entry_feat = efeat;
@@ -416,8 +450,12 @@ cudaError_t learn_models(const LearnInputs& in, LearnOutputs* out) {
     e = cudaMemsetAsync(a.counter, 0, 4, st);
     if (e == cudaSuccess) e = launch_search(SONG_KIND_L2, a, in.num_sms, st);
     if (e == cudaSuccess) {
-        entry_labels<<<(nq + 7) / 8, 256, 0, st>>>((const float*)in.base, in.ld, in.dim, d_hubs, H,
-                                                   in.nn1, nq, elab);
+        if (staged)
+            entry_labels_staged<<<(nq + 7) / 8, 256, 0, st>>>((const float*)in.base, in.ld, in.dim,
+                                                              a.ecand, in.nn1, nq, elab);
+        else
+            entry_labels<<<(nq + 7) / 8, 256, 0, st>>>((const float*)in.base, in.ld, in.dim, d_hubs,
+                                                       H, in.nn1, nq, elab);
         e = cudaGetLastError();
     }
     // 3) train the entry model

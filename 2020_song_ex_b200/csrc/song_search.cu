@@ -1112,7 +1112,48 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         }
     }
     if constexpr (LM > 0) {
-        if (a.n_hubs > 0 && !given_seeds) {
+        if (a.ecand != nullptr && !given_seeds) {
+            // entry stage: this query's kEntryK nearest hubs (nearest first) from the
+            // tensor-core kernel; the entry model re-scores them, or without a model
+            // the nearest N_MULTIPROBE become the entry points
+            const int64_t eo = (int64_t)qid * kEntryK;
+            const int hub = lane < kEntryK ? __ldg(a.ecand + eo + lane) : -1;
+            const float hd = hub >= 0 ? __ldg(a.edist + eo + lane) : INFINITY;
+            float dmin = hd;
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, w));
+            const float rel = hub >= 0 ? hd / fmaxf(dmin, 1e-30f) : 0.0f;
+            const int valid = __popc(__ballot_sync(FULL, hub >= 0));
+            n_seeds = a.n_multiprobe < valid ? a.n_multiprobe : valid;
+            if (n_seeds > 32) n_seeds = 32;
+            if (LM == 1 && a.tr_entry_feat != nullptr && lane < kFeat)
+                a.tr_entry_feat[(int64_t)qid * kFeat + lane] = hub >= 0 ? fminf(rel, 64.0f) * (1.0f / 64.0f) : 1.0f;
+            if (a.entry_w != nullptr) {
+                float f[kFeat];
+#pragma unroll
+                for (int i = 0; i < kFeat; ++i) {
+                    const float ri = __shfl_sync(FULL, rel, i);
+                    const int hi = __shfl_sync(FULL, hub, i);
+                    f[i] = hi >= 0 ? fminf(ri, 64.0f) * (1.0f / 64.0f) : 1.0f;
+                }
+                const float z = mlp_warp(a.entry_w, f, kEntryK, lane);
+                bool used = false;
+                for (int s2 = 0; s2 < n_seeds; ++s2) {  // candidates by decreasing score
+                    const unsigned key = (hub >= 0 && !used) ? fkey(z) : 0u;
+                    const unsigned mk = __reduce_max_sync(FULL, key);
+                    const int win = __ffs(__ballot_sync(FULL, hub >= 0 && !used && key == mk)) - 1;
+                    const int h = __shfl_sync(FULL, hub, win);
+                    if (lane == s2) seed_id = h;
+                    if (lane == win) used = true;
+                }
+            } else {
+                seed_id = lane < n_seeds ? hub : -1;
+            }
+            if (n_seeds < 1) {  // no hub at all: the reference's entry points
+                n_seeds = a.n_multiprobe;
+                seed_id = -1;
+            }
+        } else if (a.n_hubs > 0 && !given_seeds) {
             const int hub = lane < a.n_hubs ? __ldg(a.hubs + lane) : -1;
             const unsigned HN = __ballot_sync(FULL, hub >= 0);
             const float hd = distances(hub, HN);
@@ -1552,8 +1593,8 @@ int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a) {
     return a->warp_smem;
 }
 
-cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStream_t st,
-                         int* warps_out) {
+cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, int reserve_sms,
+                         cudaStream_t st, int* warps_out) {
     using ServeFn = void (*)(const ServeArgs);
     ServeFn fn;
     const SearchArgs& a = s.base;
@@ -1561,14 +1602,27 @@ cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStre
     else if (a.prec == SONG_PREC_FP8) fn = serve_kernel<0, SONG_PREC_FP8>;
     else if (a.dim <= 128 && a.dim > 64) fn = serve_kernel<4, 0>;
     else fn = serve_kernel<0, 0>;
-    int dev = 0, optin = 0;
+    int dev = 0, optin = 0, smem_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     if (e != cudaSuccess) return e;
-    int warps = 8;
-    while (warps > 1 && (size_t)warps * a.warp_smem > (size_t)optin / 4) warps >>= 1;
-    const size_t smem = (size_t)warps * a.warp_smem;
-    if (smem > (size_t)optin) return cudaErrorInvalidConfiguration;
+    int warps;
+    size_t smem;
+    if (reserve_sms > 0 && reserve_sms < num_sms) {
+        // Leave reserve_sms SMs free for the batched entry stage: one CTA of up
+        // to 16 warps per SM, its shared memory padded past half of the SM so
+        // that no SM can hold two, on num_sms - reserve_sms SMs.
+        warps = 16;
+        while (warps > 1 && (size_t)warps * a.warp_smem > (size_t)optin) warps >>= 1;
+        smem = std::max<size_t>((size_t)warps * a.warp_smem, (size_t)smem_sm / 2 + 1024);
+        if (smem > (size_t)optin) return cudaErrorInvalidConfiguration;
+    } else {
+        warps = 8;
+        while (warps > 1 && (size_t)warps * a.warp_smem > (size_t)optin / 4) warps >>= 1;
+        smem = (size_t)warps * a.warp_smem;
+        if (smem > (size_t)optin) return cudaErrorInvalidConfiguration;
+    }
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -1576,6 +1630,7 @@ cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, cudaStre
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid = per_sm * num_sms;
+    if (reserve_sms > 0 && reserve_sms < num_sms) grid = num_sms - reserve_sms;  // per_sm is 1
     if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
     fn<<<grid, warps * 32, smem, st>>>(s);
     if (warps_out) *warps_out = grid * warps;

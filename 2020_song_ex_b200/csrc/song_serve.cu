@@ -40,14 +40,20 @@ struct song_server {
     float* h_dist = nullptr;           // mapped [slots x max_k]
     song_query_trace* h_trace = nullptr;  // mapped [slots]
     long long* h_done = nullptr;       // mapped [slots]
+    int32_t* d_scand = nullptr;        // entry-stage candidates per slot (learned model with hubs)
+    float* d_sdist = nullptr;
+    void* d_split = nullptr;           // the entry stage's split scratch
     cudaStream_t kst = nullptr, cst = nullptr;
     cudaEvent_t kdone = nullptr;
+    cudaEvent_t pubdone = nullptr;  // the last publish's copies (and entry stage) are done
     bool launched = false;
     long long next = 0;  // next ticket
     std::mutex mu;
 };
 
 namespace {
+
+constexpr int kEntrySms = 8;  // SMs the serving kernel leaves to the entry stage
 
 song_status cuda_err(cudaError_t e, const char* what) {
     std::string m = std::string(what) + ": " + cudaGetErrorString(e);
@@ -71,7 +77,10 @@ bool slot_free(const song_server* v, long long t) {
 // (Re)launch the persistent kernel if it is not running.
 song_status ensure_running(song_server* v) {
     if (v->launched && cudaEventQuery(v->kdone) == cudaErrorNotReady) return SONG_OK;
-    cudaError_t e = song::launch_serve(v->s, v->num_sms, v->cfg.max_ctas, v->kst, &v->warps);
+    // with an entry stage, some SMs stay free for its kernel (launched on the copy
+    // stream while this persistent kernel runs)
+    const int reserve = v->d_scand != nullptr ? kEntrySms : 0;
+    cudaError_t e = song::launch_serve(v->s, v->num_sms, v->cfg.max_ctas, reserve, v->kst, &v->warps);
     if (e != cudaSuccess) return cuda_err(e, "serve launch");
     SRV_CUDA(cudaEventRecord(v->kdone, v->kst), "event");
     v->launched = true;
@@ -89,6 +98,9 @@ void free_server(song_server* v) {
     if (v->cst) cudaStreamSynchronize(v->cst);
     cudaFree(v->d_ring);
     cudaFree(v->d_ctrl);
+    cudaFree(v->d_scand);
+    cudaFree(v->d_sdist);
+    cudaFree(v->d_split);
     cudaFreeHost(v->h_stage);
     cudaFreeHost(v->h_tailbuf);
     cudaFreeHost(v->h_stop);
@@ -97,6 +109,7 @@ void free_server(song_server* v) {
     cudaFreeHost(v->h_trace);
     cudaFreeHost(v->h_done);
     if (v->kdone) cudaEventDestroy(v->kdone);
+    if (v->pubdone) cudaEventDestroy(v->pubdone);
     if (v->kst) cudaStreamDestroy(v->kst);
     if (v->cst) cudaStreamDestroy(v->cst);
     delete v;
@@ -132,12 +145,22 @@ song_status publish(song_server* v, long long t0, const float* q, int n, const i
                                  v->h_stage + (size_t)slot * v->slot_bytes,
                                  (size_t)run * v->slot_bytes, cudaMemcpyHostToDevice, v->cst),
                  "request copy");
+        if (v->d_scand != nullptr)  // the entry stage for these slots, before the tail is published
+            SRV_CUDA(song::index_entry(v->idx,
+                                       reinterpret_cast<const float*>(v->d_ring + (size_t)slot * v->slot_bytes +
+                                                                      song::kServeHeader),
+                                       v->slot_bytes / 4, (int)run,
+                                       v->d_scand + (size_t)slot * song::kEntryK,
+                                       v->d_sdist + (size_t)slot * song::kEntryK, v->cst,
+                                       v->d_split),
+                     "entry stage");
         t += run;
     }
     const int last = (int)((t0 + n - 1) % v->slots);
     v->h_tailbuf[last] = t0 + n;
     SRV_CUDA(cudaMemcpyAsync(v->d_ctrl + 1, v->h_tailbuf + last, 8, cudaMemcpyHostToDevice, v->cst),
              "tail copy");
+    SRV_CUDA(cudaEventRecord(v->pubdone, v->cst), "event");
     return ensure_running(v);
 }
 
@@ -199,9 +222,15 @@ song_status song_server_create(song_index* index, const song_server_config* cfg,
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_dist, nk * 4, cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_trace, (size_t)v->slots * sizeof(song_query_trace), cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostAlloc(&v->h_done, (size_t)v->slots * 8, cudaHostAllocMapped);
+    if (e == cudaSuccess && song::index_model_staged(index)) {
+        e = cudaMalloc(&v->d_scand, (size_t)v->slots * song::kEntryK * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&v->d_sdist, (size_t)v->slots * song::kEntryK * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&v->d_split, song::entry_split_scratch_bytes());
+    }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&v->kst, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&v->cst, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&v->kdone, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&v->pubdone, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         song_status s2 = cuda_err(e, "server allocation");
         free_server(v);
@@ -223,6 +252,8 @@ song_status song_server_create(song_index* index, const song_server_config* cfg,
     s.res_trace = v->h_trace;
     s.res_done = v->h_done;
     s.last_claim = v->d_ctrl + 3;
+    s.scand = v->d_scand;
+    s.sdist = v->d_sdist;
     s.idle_ns = (long long)cfg->idle_exit_us * 1000;
     s.sleep_ns = 2000;
     // hard bound: 64x the polls the idle time allows at the longest backoff
@@ -296,10 +327,13 @@ song_status song_server_run_poisson(song_server* v, const float* queries, int nq
     const auto t0 = clk::now();
     double last = 0.0;
     long long spins = 0;
-    // Arrivals are published in small batches: once 16 are pending or the
-    // oldest has waited 10 us (each publish is two stream-ordered copies).
-    constexpr int kBatch = 16;
-    constexpr double kWindow = 10e-6;
+    // Continuous batching of arrivals: a batch is published once the oldest
+    // pending request has waited 20 us and the previous publish (its copies
+    // and, with a learned entry stage, that stage's kernels) has finished, or
+    // at once when 128 are pending (one tile of the entry stage).  Under load
+    // the batches grow instead of the publishes queueing up.
+    constexpr int kBatch = 128;
+    constexpr double kWindow = 20e-6;
     while (ndone < nq) {
         const double now = std::chrono::duration<double>(clk::now() - t0).count();
         int m = 0;
@@ -309,8 +343,10 @@ song_status song_server_run_poisson(song_server* v, const float* queries, int nq
             if (tk - first >= v->slots && !seen[tk - first - v->slots]) break;
             ++m;
         }
+        if (m > kBatch) m = kBatch;
         const bool last_batch = sub + m == nq;
-        if (m > 0 && (m >= kBatch || last_batch || now - arrive[sub] >= kWindow)) {
+        const bool idle = cudaEventQuery(v->pubdone) != cudaErrorNotReady;
+        if (m > 0 && (m >= kBatch || (idle && (last_batch || now - arrive[sub] >= kWindow)))) {
             song_status st = publish(v, first + sub, queries + (size_t)sub * v->dim, m,
                                      ks ? ks + sub : nullptr, efs ? efs + sub : nullptr,
                                      flags ? flags + sub : nullptr);

@@ -53,7 +53,9 @@ BLOCK_SIZE = 32
 TARGET_RECALL = 0.95
 EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 512, 640, 768, 1024)
 BF_SWEEP = (256, 512, 1024)
-LEARN_THRESHOLDS = (0.8, 0.85, 0.9, 0.95, 0.98)
+LEARN_THRESHOLDS = (0.8, 0.9, 0.95, 0.98, 1.0)   # 1.0: entry stage alone, no learned stop
+LEARN_EFS = (96, 160)                              # queue sizes the models are trained at
+LEARN_SWEEP_EFS = {96: (64, 96, 128), 160: (160, 192, 256)}
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
 
 
@@ -343,17 +345,17 @@ def run_ours(args, ws, rank, local):
             query_seed=SEED + 104729 + rank).queries
         nn1, _ = gtm.knn(base, train, 1)
         torch.cuda.empty_cache()
-        song.set_precision(g, song.PREC_BF16)
         lcurve, lbest, learn_s, reps, blobs = [], None, 0.0, {}, {}
-        for lef in sorted({ef, min(1024, (ef * 3) // 2)}):
+        prec = song.PREC_FP32  # the byte rows (exact for these vectors) are read either way
+        for tef in LEARN_EFS:
             tl0 = time.time()
-            reps[lef] = song.learn(g, torch.from_numpy(train).to(dev), ntrain,
+            reps[tef] = song.learn(g, torch.from_numpy(train).to(dev), ntrain,
                                    torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(dev),
-                                   song.LearnParams(k=K, ef=lef))
+                                   song.LearnParams(k=K, ef=tef))
             torch.cuda.synchronize()
             learn_s += time.time() - tl0
-            blobs[lef] = song.get_model(g)
-            for prec in (song.PREC_FP32, song.PREC_BF16):
+            blobs[tef] = song.get_model(g)
+            for lef in LEARN_SWEEP_EFS[tef]:
                 for thr in LEARN_THRESHOLDS:
                     opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr)
                     song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
@@ -365,18 +367,19 @@ def run_ours(args, ws, rank, local):
                     ms = e0.elapsed_time(e1)
                     rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
                     trl = d_tr.cpu().numpy()
-                    pt = {"ef": lef, "precision": "bf16" if prec == song.PREC_BF16 else "fp32",
-                          "threshold": thr, "recall": round(rec, 4), "qps": round(NQ / ms * 1e3),
+                    pt = {"ef": lef, "trained_ef": tef, "threshold": thr, "recall": round(rec, 4),
+                          "qps": round(NQ / ms * 1e3),
                           "mean_expanded": round(float(trl[:, 2].mean()), 1),
+                          "mean_distance_evals": round(float(trl[:, 5].mean()), 1),
                           "learned_stop_rate": round(float((trl[:, 11] == 2).mean()), 3)}
                     lcurve.append(pt)
                     if rec >= TARGET_RECALL and (lbest is None or pt["qps"] > lbest["qps"]):
                         lbest = pt
         if lbest is not None:
             lef = lbest["ef"]
-            song.set_model(g, blobs[lef])
-            rep = reps[lef]
-            lprec = song.PREC_BF16 if lbest["precision"] == "bf16" else song.PREC_FP32
+            song.set_model(g, blobs[lbest["trained_ef"]])
+            rep = reps[lbest["trained_ef"]]
+            lprec = prec
             lopts = song.SearchOpts(precision=lprec, learned=True, stop_threshold=lbest["threshold"])
             n0 = song.launch_count()
             lms, lkern, _ = timed_device(
@@ -387,8 +390,9 @@ def run_ours(args, ws, rank, local):
             ids_l = d_ids.cpu().numpy()
             song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
             stream.synchronize()
-            l_bytes = float(bytes_per_query(d_tr.cpu().numpy(), K,
-                                            row_bytes if lprec == song.PREC_FP32 else DIM * 2).sum())
+            # gathered rows + the entry stage's hub tiles (4096 x 128 BF16 per 128 queries)
+            l_bytes = float(bytes_per_query(d_tr.cpu().numpy(), K, row_bytes).sum()) + \
+                (NQ + 127) // 128 * 4096 * DIM * 2
             copts = lopts._c()
 
             def host_learned():
@@ -400,9 +404,9 @@ def run_ours(args, ws, rank, local):
 
             l_e2e_s = timed_host(torch, dist, ws, dev, args.steps, args.warmup, host_learned)
             learned = {
-                "form": f"{lbest['precision'].upper()} rows + learned entry/stop"
-                        + (" (BF16 is exact for these integer vectors)" if lbest["precision"] == "bf16" else ""),
-                "precision": lbest["precision"], "threshold": lbest["threshold"], "ef": lef,
+                "form": "tensor-core entry stage (4096 hubs) + learned entry/stop model, byte rows",
+                "precision": "u8 rows (exact for these integer vectors)" if row_bytes < DIM * 4 else "fp32",
+                "threshold": lbest["threshold"], "ef": lef, "trained_ef": lbest["trained_ef"],
                 "qps": round(ws * NQ * args.steps / (lms / 1e3), 1),
                 "e2e_qps": round(ws * NQ * args.steps / l_e2e_s, 1),
                 "recall_at_10": round(float(ds.recall_at_k(ids_l, gt, K).mean()), 4),
@@ -447,7 +451,7 @@ def run_ours(args, ws, rank, local):
             la = learned["algorithmic_bytes_per_launch"] / (learned["kernel_ms_avg"] / 1e3) / 1e9
             lt, lsrc = ncu_traffic(learned["ef"], best["bf_words"], form="learned")
             roof_learned = {
-                "kernel": "learned search_kernel<0,4,1,0,2> (entry + stop models)",
+                "kernel": "learned search_kernel<0,4,1,0,2> (entry + stop models) after entry_kernel",
                 "bound": "hbm", "achieved": round(la, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(la / peak, 4), "peak_kind": peak_kind,
                 "traffic": lt, "traffic_source": lsrc,
@@ -457,7 +461,7 @@ def run_ours(args, ws, rank, local):
         value = learned["qps"] if use_learned else plain_qps
         e2e_v = learned["e2e_qps"] if use_learned else plain_e2e
         out = {
-            "metric": "QPS at recall@10>=0.95 (fastest form: plain bit-exact or BF16 + learned entry/stop)",
+            "metric": "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or tensor-core entry + learned stop)",
             "value": round(value, 1),
             "unit": "queries/s",
             "n_gpus": ws,
@@ -467,7 +471,7 @@ def run_ours(args, ws, rank, local):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": (learned["precision"] if use_learned else "f32").replace("fp32", "f32"),
+            "dtype": "u8" if row_bytes < DIM * 4 else "f32",
             "data": "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)",
             "config": {
                 "workload": WORKLOAD, "n": N_BASE, "dim": DIM, "nq_per_gpu": NQ, "k": K,

@@ -161,6 +161,22 @@ song_status song_gpu_search_hamming(song_index* index, const uint32_t* queries, 
                                     song_query_trace* traces, song_timing* timing);
 
 /*
+ * The reference's CPU search, Graph::search (graph.h:33-115), on the GPU:
+ * exact visited set, unbounded frontier and top-ef ordered by (distance,
+ * id), distances summed in dimension order.  For the same graph, queries
+ * and ef the ids (worst-first, as Graph::search returns them, -1 padded to
+ * k) and all twelve QueryTrace counters equal the reference's bit for bit.
+ * ef_search is raised to k (graph.h:36); it must be 1..1024 and at least
+ * N_MULTIPROBE.  L2 indexes.  Host buffers, synchronous; the device form is
+ * asynchronous on `stream`.
+ */
+song_status song_graph_search(song_index* index, const float* queries, int nq, int k,
+                              int ef_search, int32_t* ids, song_query_trace* traces);
+song_status song_graph_search_device(song_index* index, const float* d_queries, int nq, int k,
+                                     int ef_search, int32_t* d_ids, song_query_trace* d_traces,
+                                     void* stream);
+
+/*
  * Device-resident search: d_queries (FP32 or u32 codes, by index kind),
  * d_ids[nq x k] and d_traces (nullable) are device pointers; the call is
  * asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).
@@ -288,6 +304,8 @@ typedef struct song_learn_params {
     int batch;           /* minibatch (default 4096)                                       */
     float lr;            /* Adam learning rate (default 2e-3)                              */
     unsigned seed;
+    int entry_hubs;      /* hub set of the tensor-core entry stage (default 4096; dim <= 288).
+                            0: the entry model scores 24 farthest-point hubs instead   */
 } song_learn_params;
 
 typedef struct song_learn_report {

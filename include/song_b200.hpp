@@ -5,6 +5,8 @@
 //   HashKernelGraph  hashKernelGraph.h:22-126 (codes + adj)
 //   gpu_search       kernalGraph.h:307-382 and hashKernelGraph.h:360-435
 //   build_kernel_graph kernalGraph.h:140-149 (here: the batched GPU build)
+//   graph_search     graph.h:33-115 (Graph::search's results, on the GPU)
+//   BitHash          bitHash.h:17-56 (projection on the GPU)
 //   GpuSearchTrace / QueryTrace telemetry.h:5-41
 // The compile-time constants of config.h become a song_params value (the
 // reference defaults unless given).  Results, tie order and QueryTrace
@@ -172,6 +174,45 @@ inline std::vector<int> gpu_search(const HashKernelGraph& g, const uint32_t* que
     if (trace) detail::fill_trace(trace, t, nq, N_MULTIQUERY);
     return ids;
 }
+
+// Graph::search (graph.h:33-115) for nq queries, computed on the GPU with the
+// reference's CPU results: each entry is what Graph::search returns for that
+// query (the best min(k, found) ids, worst first).  ef_search <= 0 selects k.
+inline std::vector<std::vector<int>> graph_search(const KernelGraph& g, const float* queries,
+                                                  int nq, int k, int ef_search = 0,
+                                                  std::vector<QueryTrace>* traces = nullptr) {
+    if (!g.index()) throw std::runtime_error("song_b200: graph not uploaded");
+    std::vector<int32_t> ids((size_t)nq * k);
+    std::vector<QueryTrace> tr((size_t)nq);
+    check(song_graph_search(g.index(), queries, nq, k, ef_search, ids.data(), tr.data()));
+    std::vector<std::vector<int>> out((size_t)nq);
+    for (int i = 0; i < nq; ++i)
+        out[(size_t)i].assign(ids.begin() + (size_t)i * k, ids.begin() + (size_t)i * k + tr[(size_t)i].result_count);
+    if (traces) *traces = std::move(tr);
+    return out;
+}
+
+// BitHash (bitHash.h:17-56): the projection matrix drawn as the reference's
+// constructor draws it; project / project_all run on the GPU and return the
+// reference's codes bit for bit.  hash_bits is config.h's hash_bits.
+struct BitHash {
+    int dim;
+    int hash_bits;
+    std::vector<float> R;  // [hash_bits x dim]
+
+    explicit BitHash(int dim_, unsigned seed = 42, int hash_bits_ = 256)
+        : dim(dim_), hash_bits(hash_bits_), R((size_t)hash_bits_ * dim_) {
+        check(song_bithash_matrix(dim, hash_bits, seed, R.data()));
+    }
+    void project(const float* vec, uint32_t* out) const {
+        check(song_bithash_project(R.data(), dim, hash_bits, vec, 1, out));
+    }
+    std::vector<uint32_t> project_all(const float* data, int n) const {
+        std::vector<uint32_t> out((size_t)n * (hash_bits / 32));
+        check(song_bithash_project(R.data(), dim, hash_bits, data, n, out.data()));
+        return out;
+    }
+};
 
 // build_kernel_graph (kernalGraph.h:140-149), built on the GPU in batches.
 inline KernelGraph build_kernel_graph(std::vector<float> data, int n, int dim,

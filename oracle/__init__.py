@@ -64,6 +64,9 @@ def lib() -> C.CDLL:
             _u32p, C.c_int64, C.c_int, _i32p, C.c_int, _u32p, C.c_int, C.c_int, C.c_int,
             C.c_int, C.c_int, C.c_int, C.c_int, _i32p, C.c_void_p, C.c_int]
         L.oracle_search_hamming.restype = C.c_int
+        L.oracle_graph_search.argtypes = [_f32p, C.c_int64, C.c_int, _i32p, C.c_int, _f32p,
+                                          C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p]
+        L.oracle_graph_search.restype = None
         L.oracle_bithash_matrix.argtypes = [C.c_int, C.c_int, C.c_uint, _f32p]
         L.oracle_bithash_matrix.restype = None
         L.oracle_bithash_project.argtypes = [_f32p, C.c_int, C.c_int, _f32p, C.c_int64, _u32p]
@@ -111,6 +114,20 @@ def search_hamming(codes, adj, block_size, qcodes, k, ef, pq_size=50, bf_words=2
         threads or os.cpu_count() or 1)
     if rc != 0:
         raise ValueError("oracle_search_hamming: invalid arguments")
+    return ids, trace
+
+
+def graph_search(data, adj, block_size, queries, k, ef, n_multiprobe=4):
+    """Graph::search (graph.h:33-115) restated: ids worst-first (-1 padded) and traces."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    queries = np.ascontiguousarray(queries, dtype=np.float32)
+    adj = np.ascontiguousarray(adj, dtype=np.int32).reshape(-1)
+    n, dim = data.shape
+    nq = queries.shape[0]
+    ids = np.empty((nq, k), dtype=np.int32)
+    trace = np.zeros((nq, 12), dtype=np.int32)
+    lib().oracle_graph_search(data, n, dim, adj, block_size, queries, nq, k, ef, n_multiprobe,
+                              ids, trace)
     return ids, trace
 
 

@@ -25,6 +25,10 @@
 #include <thread>
 #include <atomic>
 #include <vector>
+#include <queue>
+#include <unordered_set>
+#include <algorithm>
+#include <utility>
 
 namespace {
 
@@ -277,6 +281,83 @@ int oracle_search_hamming(const uint32_t* codes, int64_t n, int words, const int
                           int32_t* trace, int nthreads) {
     Args a{codes, n, words, true, adj, block_size, k, ef, pq_size, bf_words, bf_nhash, n_multiprobe};
     return run(a, queries, nq, ids, trace, nthreads);
+}
+
+// Graph::search (graph.h:33-115), restated: exact visited set, min-heap
+// frontier and max-heap top-ef of (distance, id) pairs, l2 summed in
+// dimension order (distance.h:5-12), seeds p*n/N_MULTIPROBE, results
+// worst-first.  ids[nq*k] (-1 padded) and trace[nq*12].
+void oracle_graph_search(const float* base, int64_t n, int dim, const int32_t* adj,
+                         int block_size, const float* queries, int nq, int k, int ef,
+                         int n_multiprobe, int32_t* ids, int32_t* trace) {
+    using P = std::pair<float, int>;
+    if (ef < k) ef = k;  // graph.h:36
+    for (int qi = 0; qi < nq; ++qi) {
+        const float* q = queries + (size_t)qi * dim;
+        auto l2 = [&](int v) {  // distance.h:5-12
+            const float* b = base + (size_t)v * dim;
+            float s = 0.0f;
+            for (int i = 0; i < dim; ++i) {
+                float d = q[i] - b[i];
+                float dd = d * d;
+                s = s + dd;
+            }
+            return s;
+        };
+        Trace t{};
+        std::priority_queue<P, std::vector<P>, std::greater<P>> fr;
+        std::priority_queue<P> topk;
+        std::unordered_set<int> visited;
+        for (int p = 0; p < n_multiprobe; ++p) {  // graph.h:47-62
+            const int ep = (int)((uint64_t)p * (uint64_t)n / (uint64_t)n_multiprobe);
+            if (visited.count(ep)) continue;
+            const float d = l2(ep);
+            fr.push({d, ep});
+            topk.push({d, ep});
+            visited.insert(ep);
+            t.seed_count++; t.visited_nodes++; t.distance_evals++;
+            t.frontier_pushes++; t.result_updates++;
+            t.peak_frontier = std::max(t.peak_frontier, (int)fr.size());
+            t.peak_results = std::max(t.peak_results, (int)topk.size());
+        }
+        while (!fr.empty()) {  // graph.h:64-104
+            const P cur = fr.top();
+            fr.pop();
+            t.expanded_nodes++;
+            if ((int)topk.size() == ef && cur.first > topk.top().first) {
+                t.early_stopped = 1;
+                break;
+            }
+            std::vector<int> cands;
+            for (int j = 0; j < block_size; ++j) {
+                t.neighbor_slots_scanned++;
+                const int v = adj[(size_t)cur.second * block_size + j];
+                if (v < 0 || visited.count(v)) continue;
+                visited.insert(v);
+                cands.push_back(v);
+                t.visited_nodes++; t.candidate_nodes++;
+            }
+            std::vector<float> dists(cands.size());
+            for (size_t i = 0; i < cands.size(); ++i) { dists[i] = l2(cands[i]); t.distance_evals++; }
+            for (size_t i = 0; i < cands.size(); ++i) {
+                fr.push({dists[i], cands[i]});
+                t.frontier_pushes++;
+                t.peak_frontier = std::max(t.peak_frontier, (int)fr.size());
+                if ((int)topk.size() < ef || dists[i] < topk.top().first) {
+                    topk.push({dists[i], cands[i]});
+                    if ((int)topk.size() > ef) topk.pop();
+                    t.result_updates++;
+                    t.peak_results = std::max(t.peak_results, (int)topk.size());
+                }
+            }
+        }
+        while ((int)topk.size() > k) topk.pop();  // graph.h:106-112
+        int c = 0;
+        while (!topk.empty()) { ids[(size_t)qi * k + c++] = topk.top().second; topk.pop(); }
+        t.result_count = c;
+        for (int i = c; i < k; ++i) ids[(size_t)qi * k + i] = -1;
+        std::memcpy(trace + (size_t)qi * 12, &t, sizeof t);
+    }
 }
 
 // BitHash(dim, seed) (bitHash.h:23-27): R[hash_bits x dim] from std::mt19937

@@ -3,18 +3,23 @@
 // the adjacency, upload_to_gpu, gpu_search with a GpuSearchTrace.
 // Input file: int32 n, dim, nq, k, ef, block_size, then data[n*dim] f32,
 // adj[n*block_size] i32, queries[nq*dim] f32.  Output: ids[nq*k] i32 then
-// the traces [nq*12] i32.  Exit 2 with the library's message on failure.
+// the traces [nq*12] i32.  With a third argument "extras" it then appends
+// Graph::search's results through graph_search (ids [nq*k] i32, -1 padded,
+// traces [nq*12] i32) and BitHash(dim, 42, 256).project_all of the queries
+// ([nq*8] u32).  Exit 2 with the library's message on failure.
 #include <cstdio>
 #include <exception>
+#include <string>
 #include <vector>
 
 #include "song_b200.hpp"
 
 int main(int argc, char** argv) {
-    if (argc != 3) {
-        std::fprintf(stderr, "usage: %s input.bin output.bin\n", argv[0]);
+    if (argc != 3 && argc != 4) {
+        std::fprintf(stderr, "usage: %s input.bin output.bin [extras]\n", argv[0]);
         return 1;
     }
+    const bool extras = argc == 4 && std::string(argv[3]) == "extras";
     std::FILE* f = std::fopen(argv[1], "rb");
     if (!f) return 1;
     int h[6];
@@ -40,6 +45,19 @@ int main(int argc, char** argv) {
         std::FILE* o = std::fopen(argv[2], "wb");
         std::fwrite(ids.data(), 4, ids.size(), o);
         std::fwrite(trace.queries.data(), sizeof(song_b200::QueryTrace), trace.queries.size(), o);
+        if (extras) {
+            std::vector<song_b200::QueryTrace> gtr;
+            std::vector<std::vector<int>> res = song_b200::graph_search(g, q.data(), nq, k, ef, &gtr);
+            for (const auto& r : res) {
+                std::vector<int> row(r);
+                row.resize((size_t)k, -1);
+                std::fwrite(row.data(), 4, row.size(), o);
+            }
+            std::fwrite(gtr.data(), sizeof(song_b200::QueryTrace), gtr.size(), o);
+            song_b200::BitHash bh(dim);
+            std::vector<uint32_t> codes = bh.project_all(q.data(), nq);
+            std::fwrite(codes.data(), 4, codes.size(), o);
+        }
         std::fclose(o);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "%s\n", e.what());

@@ -57,3 +57,23 @@ def test_shim_matches_oracle(cuda, shim_bin, ds, oracle, tmp_path):
     oids, otr = oracle.search_l2(m.base, adj, 32, m.queries, 10, 64, pq_size=512, bf_words=256)
     np.testing.assert_array_equal(ids, oids)
     np.testing.assert_array_equal(tr, otr)
+
+
+@pytest.mark.gpu
+def test_shim_graph_search_and_bithash(cuda, shim_bin, ds, oracle, tmp_path):
+    """graph_search (Graph::search's results) and BitHash through the C++ shim."""
+    m = ds.angular_mixture(2500, 60, dim=64, n_comp=8, seed=9)
+    adj = knn_graph(m.base, 32, 28, seed=4)
+    inp, outp = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    _write_case(inp, m.base, adj, m.queries, 10, 40)
+    subprocess.check_call([shim_bin, inp, outp, "extras"])
+    raw = np.fromfile(outp, dtype=np.int32)
+    o = 60 * 10 + 60 * 12
+    gids = raw[o:o + 600].reshape(60, 10)
+    gtr = raw[o + 600:o + 600 + 720].reshape(60, 12)
+    codes = raw[o + 1320:].view(np.uint32).reshape(60, 8)
+    oids, otr = oracle.graph_search(m.base, adj, 32, m.queries, 10, 40)
+    np.testing.assert_array_equal(gids, oids)
+    np.testing.assert_array_equal(gtr, otr)
+    np.testing.assert_array_equal(codes, oracle.bithash_project(oracle.bithash_matrix(64, 256, 42),
+                                                                 m.queries))

@@ -9,6 +9,8 @@ tcgen05 tensor-core kernel (BF16 operands, FP32 accumulation in TMEM).
   no hub is missed by more than that tolerance.
 * Ragged shapes: dims that are not multiples of 16, hub counts that are not
   whole tiles or below 24, query counts that are not whole 128-query tiles.
+  Batches of up to 128 queries spread the hub tiles over several CTAs and
+  merge their lists; the result must not change.
 """
 import numpy as np
 import pytest
@@ -37,7 +39,8 @@ def _run(song, base, hubs, q):
 
 
 @pytest.mark.parametrize("n,dim,nh,nq", [(20000, 128, 1000, 300), (3000, 37, 700, 129),
-                                         (2000, 64, 10, 5), (5000, 96, 256, 128)])
+                                         (2000, 64, 10, 5), (5000, 96, 256, 128),
+                                         (30000, 128, 4096, 100), (9000, 80, 2100, 1)])
 def test_integer_vectors_exact(cuda, song, ds, n, dim, nh, nq):
     m = ds.int_mixture(n, nq, dim=dim, n_comp=16, seed=n + dim)
     rng = np.random.default_rng(dim)

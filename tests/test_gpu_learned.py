@@ -24,7 +24,7 @@ def test_training_gradients_match_oracle(cuda, song, out, loss_kind):
     np.testing.assert_allclose(g, go, rtol=2e-4, atol=2e-6)
 
 
-def _setup(song, ds, n=30000, nq=400, ntrain=4000):
+def _setup(song, ds, n=30000, nq=400, ntrain=4000, entry_hubs=4096):
     torch = importlib.import_module("torch")
     gtm = importlib.import_module("2020_song_ex_b200.groundtruth")
     m = ds.int_mixture(n, nq, dim=128, n_comp=64, seed=61)
@@ -36,12 +36,18 @@ def _setup(song, ds, n=30000, nq=400, ntrain=4000):
     gt, _ = gtm.knn(m.base, m.queries, 10)
     rep = song.learn(g, torch.from_numpy(train).cuda(), ntrain,
                      torch.from_numpy(nn1[:, 0].copy()).cuda(),
-                     song.LearnParams(k=10, ef=128, entry_steps=600, stop_steps=1200))
+                     song.LearnParams(k=10, ef=128, entry_steps=600, stop_steps=1200,
+                                      entry_hubs=entry_hubs))
     return m, g, gt, rep
 
 
-def test_learned_models_gain_over_plain(cuda, song, ds):
-    m, g, gt, rep = _setup(song, ds)
+@pytest.mark.parametrize("entry_hubs", [4096, 0])
+def test_learned_models_gain_over_plain(cuda, song, ds, entry_hubs):
+    """entry_hubs 4096: the tensor-core entry stage proposes 24 candidates per
+    query and the entry model scores them; 0: the entry model scores 24
+    farthest-point hubs inside the search kernel."""
+    m, g, gt, rep = _setup(song, ds, entry_hubs=entry_hubs)
+    assert rep["n_hubs"] == (entry_hubs if entry_hubs else 24)
     assert rep["stop_loss_last"] < rep["stop_loss_first"]
     assert rep["entry_loss_last"] < rep["entry_loss_first"]
     assert 0.0 < rep["stop_pos_frac"] < 1.0 and rep["stop_samples"] > 0
@@ -72,3 +78,20 @@ def test_learned_models_gain_over_plain(cuda, song, ds):
     np.testing.assert_array_equal(ids_2, ids_l)
     g.close()
     g2.close()
+
+
+def test_entry_stage_cuts_work_at_equal_recall(cuda, song, ds):
+    """The entry stage's nearest hubs as entry points: at a quarter of the
+    queue size the search reaches the plain search's recall with far fewer
+    distance evaluations."""
+    m, g, gt, rep = _setup(song, ds, n=30000, nq=400, ntrain=2000)
+    nq = m.queries.shape[0]
+    tp, tl = song.GpuSearchTrace(), song.GpuSearchTrace()
+    ids_p, _ = song.gpu_search_ex(g, song.SearchOpts(), m.queries, nq, 10, 256, trace=tp)
+    ids_l, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0),
+                                  m.queries, nq, 10, 64, trace=tl)
+    rec_p = ds.recall_at_k(ids_p, gt, 10).mean()
+    rec_l = ds.recall_at_k(ids_l, gt, 10).mean()
+    assert rec_l >= rec_p - 0.01, (rec_p, rec_l)
+    assert tl.queries[:, 5].mean() < 0.6 * tp.queries[:, 5].mean()
+    g.close()
