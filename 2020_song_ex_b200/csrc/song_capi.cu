@@ -80,7 +80,8 @@ struct song_index {
     size_t ecand_cap = 0;
     float* d_edist = nullptr;
     size_t edist_cap = 0;
-    void* d_esplit = nullptr;  // split scratch of the entry stage (batches of <= 128 queries)
+    void* d_esplit = nullptr;  // split scratch of the entry stage (grown on demand)
+    size_t esplit_cap = 0;
     // learned entry / stop models
     bool has_model = false;
     bool model_staged = false;  // the entry model scores the entry stage's candidates
@@ -289,11 +290,11 @@ song_status attach_entry_hubs(song_index* x, const std::vector<int32_t>& hubs) {
 // The entry stage for nq queries at d_q: ids/dists [nq x kEntryK].
 song_status run_entry(song_index* x, const void* d_q, int nq, int32_t* d_ids, float* d_d,
                       cudaStream_t st) {
-    if (x->d_esplit == nullptr)
-        SONG_CUDA(cudaMalloc(&x->d_esplit, song::entry_split_scratch_bytes()), "entry split scratch");
+    SONG_CUDA(grow(&x->d_esplit, &x->esplit_cap, song::entry_split_scratch_bytes(nq, x->num_sms)),
+              "entry split scratch");
     cudaError_t e = song::launch_entry((const float*)d_q, x->dim, nq, x->dim, x->d_entry_tiles,
                                        x->d_entry_norm, x->d_entry_ids, x->entry_hpad, d_ids, d_d,
-                                       x->d_err, st, x->d_esplit);
+                                       x->d_err, st, x->d_esplit, x->esplit_cap, x->num_sms);
     if (e != cudaSuccess) return cuda_fail(e, "entry launch");
     return SONG_OK;
 }
@@ -512,10 +513,10 @@ song_status server_args(song_index* x, const song_search_opts* opts, int max_k, 
 int index_pq_size(const song_index* x) { return x ? x->p.pq_size : 0; }
 bool index_model_staged(const song_index* x) { return x && x->has_model && x->model_staged; }
 cudaError_t index_entry(song_index* x, const float* d_q, int qld, int nq, int32_t* d_ids,
-                        float* d_d, cudaStream_t st, void* split_scratch) {
+                        float* d_d, cudaStream_t st, void* split_scratch, size_t split_bytes) {
     return song::launch_entry(d_q, qld, nq, x->dim, x->d_entry_tiles, x->d_entry_norm,
                               x->d_entry_ids, x->entry_hpad, d_ids, d_d, x->d_err, st,
-                              split_scratch);
+                              split_scratch, split_bytes, x->num_sms);
 }
 int index_dim(const song_index* x) { return x ? x->dim : 0; }
 bool index_has_model(const song_index* x) { return x && x->has_model; }

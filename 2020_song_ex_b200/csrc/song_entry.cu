@@ -109,7 +109,12 @@ struct EntryArgs {
 };
 
 __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
-    extern __shared__ __align__(1024) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
+    // Each thread's 32 keys of the current accumulator chunk (XOR-swizzled by
+    // thread, conflict-free), so that only the keys below its threshold are
+    // visited by the insertion loop; and the current tile's hub norms.
+    __shared__ float stage[kM * 32];
+    __shared__ float hn_s[kN];
     __shared__ __align__(8) uint64_t bar_load[2];
     __shared__ __align__(8) uint64_t bar_mma;
     __shared__ uint32_t tslot;
@@ -200,13 +205,15 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                 :: "r"(smem_addr(&bar_mma)) : "memory");
         }
+        hn_s[tid] = __ldg(a.hub_norm + (size_t)t * kN + tid);  // kN == blockDim.x
         ok = __syncthreads_and(mbar_wait(smem_addr(&bar_mma), (uint32_t)(u & 1)));
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // the MMAs have read this buffer: refill it with tile t + 2
         if (tid == 0 && t + 2 < t_end) issue_load(t + 2, buf);
-        const float* hn = a.hub_norm + (size_t)t * kN;
         const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
+        float* my = stage + tid * 32;
+        const int sw = tid & 31;
         for (int c0 = 0; c0 < kN; c0 += 32) {
             uint32_t r[32];
             asm volatile(
@@ -222,9 +229,25 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
                   "=r"(r[30]), "=r"(r[31])
                 : "r"(row + (uint32_t)c0)
                 : "memory");
+            // keys below this thread's current 24th: a 32-bit mask, then the
+            // insertion loop visits only those (the warp pays the largest count
+            // among its threads, not one pass per key any thread wants)
+            const float thr = kd[kK - 1];
+            float dv[32];
+            unsigned m = 0u;
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                const float d = fmaf(-2.0f, __uint_as_float(r[j]), __ldg(hn + c0 + j));
+                dv[j] = fmaf(-2.0f, __uint_as_float(r[j]), hn_s[c0 + j]);
+                m |= (dv[j] < thr ? 1u : 0u) << j;
+            }
+            if (m) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) my[j ^ sw] = dv[j];
+            }
+            while (m) {
+                const int j = __ffs(m) - 1;
+                m &= m - 1u;
+                const float d = my[j ^ sw];
                 if (d < kd[kK - 1]) {  // sorted insertion; equal keys keep the earlier hub first
                     const int idx = t * kN + c0 + j;
 #pragma unroll
@@ -384,12 +407,17 @@ size_t entry_smem_bytes(int dim) {
     return (size_t)kM * kp * 2 + 2 * (size_t)kN * kp * 2;
 }
 
-size_t entry_split_scratch_bytes() { return (size_t)kEntrySplits * kM * kK * 8; }
+size_t entry_split_scratch_bytes(int nq, int num_sms) {
+    const int qt = (nq + kM - 1) / kM;
+    int splits = qt <= 1 ? kEntrySplits : (2 * num_sms) / qt;
+    splits = std::max(1, std::min(kEntrySplits, splits));
+    return (size_t)splits * std::max(nq, 1) * kK * 8;
+}
 
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
-                         cudaStream_t st, void* split_scratch) {
+                         cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms) {
     if (nq <= 0) return cudaSuccess;
     if (dim > kEntryMaxDim || hpad % kN != 0 || hpad <= 0) return cudaErrorInvalidValue;
     EntryArgs a;
@@ -404,16 +432,22 @@ cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
     a.ntiles = hpad / kN;
     a.out_ids = d_out_ids;
     a.out_d = d_out_d;
-    // A single tile of queries (serving batches) spreads its hub tiles over up
-    // to kEntrySplits CTAs, merged afterwards; larger batches use one CTA per
-    // 128 queries over all tiles.
-    int splits = 1;
-    if (nq <= kM && split_scratch != nullptr) splits = std::min(kEntrySplits, a.ntiles);
+    // The hub tiles are spread over `splits` CTAs per 128 queries (about two
+    // CTAs per SM in all, up to kEntrySplits), as far as the caller's scratch
+    // holds their partial lists; the lists are merged afterwards.  The result
+    // does not depend on the split.
+    const int qt = (nq + kM - 1) / kM;
+    int splits = qt <= 1 ? kEntrySplits : (2 * num_sms) / qt;
+    splits = std::max(1, std::min(std::min(kEntrySplits, a.ntiles), splits));
+    const size_t per_split = (size_t)nq * kK * 8;
+    if (split_scratch == nullptr) splits = 1;
+    else splits = (int)std::min<size_t>((size_t)splits, split_bytes / per_split);
+    if (splits < 1) splits = 1;
     a.tiles_per_split = (a.ntiles + splits - 1) / splits;
     splits = (a.ntiles + a.tiles_per_split - 1) / a.tiles_per_split;
     a.part_key = static_cast<float*>(split_scratch);
     a.part_idx = reinterpret_cast<int32_t*>(static_cast<char*>(split_scratch) +
-                                            (size_t)kEntrySplits * kM * kK * 4);
+                                            (size_t)splits * nq * kK * 4);
     a.err = d_err;
     const size_t smem = entry_smem_bytes(dim);
     cudaError_t e = cudaFuncSetAttribute(entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

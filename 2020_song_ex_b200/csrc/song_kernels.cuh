@@ -90,14 +90,15 @@ cudaError_t build_entry_tables(const float* d_base, int ld, int dim, const int32
 // out_ids / out_d [nq x kEntryK]: each query's nearest hubs (node ids, -1 if
 // none) and squared distances, nearest first.  err is set to 2 if a bounded
 // wait gives up.
-// split_scratch (entry_split_scratch_bytes(), nullable): lets batches of up
-// to 128 queries spread the hub tiles over several CTAs (serving).
+// split_scratch (nullable, split_bytes long; entry_split_scratch_bytes(nq,
+// num_sms) is enough for the widest split) lets the hub tiles of each 128
+// queries spread over several CTAs, whose lists are merged afterwards.
 constexpr int kEntrySplits = 16;
-size_t entry_split_scratch_bytes();
+size_t entry_split_scratch_bytes(int nq, int num_sms);
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
-                         cudaStream_t st, void* split_scratch = nullptr);
+                         cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms);
 
 // Graph::search (graph.h:33-115) bit for bit (song_graphsearch.cu).
 int graph_search_frontier_cap(int ef);
@@ -220,7 +221,7 @@ bool index_has_model(const song_index* x);
 // qld floats apart.
 bool index_model_staged(const song_index* x);
 cudaError_t index_entry(song_index* x, const float* d_q, int qld, int nq, int32_t* d_ids,
-                        float* d_d, cudaStream_t st, void* split_scratch = nullptr);
+                        float* d_d, cudaStream_t st, void* split_scratch, size_t split_bytes);
 
 // Records a failure message for song_last_error() on the calling thread.
 song_status set_error(song_status status, const char* message);

@@ -961,6 +961,8 @@ __device__ __forceinline__ unsigned fkey(float x) {
 // KIND 1 = Hamming with NE uint4 of code per row.  GPL: queue groups per lane.
 // DT: SONG_PREC_FP32 (the plain, bit-exact search) or the precision form on
 // BF16 / FP8 rows (KIND 0, query in shared memory, FP32 re-rank at the end).
+// LM: 0 plain; 1 learning traces; 2 learned entry and stop; 3 learned entry
+// only (the instance for a stop model that cannot fire).
 // TM = 1: the queue ids live in this warp's TMEM lanes from column `tbase`
 // (candidates in columns tbase .. tbase+G-1, results in the next G, with G =
 // ceil(cap / 32)); the per-warp shared-memory layout then has no id arrays.
@@ -1210,7 +1212,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     break;
                 }
             }
-            if constexpr (LM > 0) {  // learned-stop checkpoint
+            if constexpr (LM == 1 || LM == 2) {  // learned-stop checkpoint
                 ss.hops_kth += 1;
                 ss.hops_best += 1;
                 const int t = tr.expanded_nodes;
@@ -1299,7 +1301,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             const int pr = q_push<false>(res, N, d, nb, lane, rows);
             tr.frontier_pushes += pf;
             tr.result_updates += pr;
-            if constexpr (LM > 0) {
+            if constexpr (LM == 1 || LM == 2) {
                 topk_insert(ss, N, d, lane);
                 ss.n_new += c;
                 ss.n_res += pr;
@@ -1347,7 +1349,7 @@ template <int KIND, int NE, int GPL, int DT, int LM>
 struct KernelShape {
     static constexpr int kTM = GPL == 1 ? 1 : 0;
     static constexpr int kThreads = kTM ? 128 : 256;
-    static constexpr int kMinBlocks = kTM ? ((LM > 0 || NE >= 8) ? 5 : 6) : 1;
+    static constexpr int kMinBlocks = kTM ? ((LM == 1 || LM == 2 || NE >= 8) ? 5 : 6) : 1;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
 };
 
@@ -1485,7 +1487,11 @@ KernelSel pick_learned(const SearchArgs& a) {
 KernelSel pick_kernel(int kind, const SearchArgs& a) {
     if (a.lm != 0) {  // learned entry/stop: L2, queues up to 1024 slots
         if (kind != SONG_KIND_L2 || a.cap > 1024) return KernelSel();
-        return a.lm == 1 ? pick_learned<1>(a) : pick_learned<2>(a);
+        if (a.lm == 1) return pick_learned<1>(a);
+        // a stop model that can never fire (none, or threshold >= 1): the entry-only
+        // instance, without the stop statistics -- the same results, less state
+        if (a.stop_w == nullptr || !(a.stop_thr < INFINITY)) return pick_learned<3>(a);
+        return pick_learned<2>(a);
     }
     if (a.cap <= 1024) return pick_gpl<1>(kind, a);
     if (a.cap <= 2048) return pick_gpl<2>(kind, a);

@@ -42,7 +42,8 @@ struct song_server {
     long long* h_done = nullptr;       // mapped [slots]
     int32_t* d_scand = nullptr;        // entry-stage candidates per slot (learned model with hubs)
     float* d_sdist = nullptr;
-    void* d_split = nullptr;           // the entry stage's split scratch
+    void* d_split = nullptr;           // the entry stage's split scratch (batches <= 128)
+    size_t split_bytes = 0;
     cudaStream_t kst = nullptr, cst = nullptr;
     cudaEvent_t kdone = nullptr;
     cudaEvent_t pubdone = nullptr;  // the last publish's copies (and entry stage) are done
@@ -152,7 +153,7 @@ song_status publish(song_server* v, long long t0, const float* q, int n, const i
                                        v->slot_bytes / 4, (int)run,
                                        v->d_scand + (size_t)slot * song::kEntryK,
                                        v->d_sdist + (size_t)slot * song::kEntryK, v->cst,
-                                       v->d_split),
+                                       v->d_split, v->split_bytes),
                      "entry stage");
         t += run;
     }
@@ -225,7 +226,8 @@ song_status song_server_create(song_index* index, const song_server_config* cfg,
     if (e == cudaSuccess && song::index_model_staged(index)) {
         e = cudaMalloc(&v->d_scand, (size_t)v->slots * song::kEntryK * 4);
         if (e == cudaSuccess) e = cudaMalloc(&v->d_sdist, (size_t)v->slots * song::kEntryK * 4);
-        if (e == cudaSuccess) e = cudaMalloc(&v->d_split, song::entry_split_scratch_bytes());
+        v->split_bytes = song::entry_split_scratch_bytes(128, v->num_sms);
+        if (e == cudaSuccess) e = cudaMalloc(&v->d_split, v->split_bytes);
     }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&v->kst, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&v->cst, cudaStreamNonBlocking);

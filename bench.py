@@ -451,7 +451,9 @@ def run_ours(args, ws, rank, local):
             la = learned["algorithmic_bytes_per_launch"] / (learned["kernel_ms_avg"] / 1e3) / 1e9
             lt, lsrc = ncu_traffic(learned["ef"], best["bf_words"], form="learned")
             roof_learned = {
-                "kernel": "learned search_kernel<0,4,1,0,2> (entry + stop models) after entry_kernel",
+                "kernel": ("entry_kernel + search_kernel<0,4,1,0,3> (entry model; the stop cannot fire)"
+                           if learned["threshold"] >= 1.0 else
+                           "entry_kernel + search_kernel<0,4,1,0,2> (entry + stop models)"),
                 "bound": "hbm", "achieved": round(la, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(la / peak, 4), "peak_kind": peak_kind,
                 "traffic": lt, "traffic_source": lsrc,
