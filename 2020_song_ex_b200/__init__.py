@@ -70,7 +70,7 @@ class _Timing(C.Structure):
 
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("rerank", C.c_int), ("learned", C.c_int),
-                ("stop_threshold", C.c_float), ("reserved", C.c_int * 4)]
+                ("stop_threshold", C.c_float), ("beam", C.c_int), ("reserved", C.c_int * 3)]
 
 
 @dataclass
@@ -81,10 +81,11 @@ class SearchOpts:
     rerank: bool = False
     learned: bool = False
     stop_threshold: float = 0.5
+    beam: int = 1  # learned search: 2 expands the two best candidates per step
 
     def _c(self) -> _Opts:
         return _Opts(int(self.precision), int(bool(self.rerank)), int(bool(self.learned)),
-                     float(self.stop_threshold))
+                     float(self.stop_threshold), int(self.beam))
 
 
 class _LearnParams(C.Structure):

@@ -364,6 +364,7 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
         a->stop_w = x->d_stop_w;
         a->ckpt_every = x->ckpt_every;
         a->min_expansions = x->min_expansions;
+        a->beam = opts->beam >= 2 ? 2 : 1;
         const float t = opts->stop_threshold;
         a->stop_thr = t <= 0.0f ? -INFINITY : (t >= 1.0f ? INFINITY : std::log(t / (1.0f - t)));
     }

@@ -1190,7 +1190,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     for (;;) {
         int limit;
         const int32_t* arow = nullptr;
-        int first = -1;  // first chunk of the adjacency row
+        const int32_t* arow2 = nullptr;  // learned search, beam 2: a second row this step
+        int first = -1, first2 = -1;      // first chunk of each adjacency row
+        int nrows = 1;
         if (seeding) {
             limit = n_seeds;  // seeds p*n/N_MULTIPROBE (kernalGraph.h:214-231)
         } else {              // expansion (kernalGraph.h:233-289)
@@ -1212,9 +1214,26 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     break;
                 }
             }
+            if constexpr (LM > 0) {
+                // Beam 2 (learned searches only; not the reference's order): the
+                // runner-up is expanded in the same step when it would not end the
+                // search, so both adjacency rows are fetched in one round trip.
+                if (a.beam > 1 && cand.sz > 0 && a.block_size <= 32) {
+                    unsigned mb2, mi2;
+                    root_min(cand, mb2, mi2);
+                    if (!(res.sz == res.cap && mb2 > wb)) {
+                        const int cn2 = q_id(cand, (int)mi2);
+                        arow2 = a.adj + (int64_t)cn2 * a.block_size;
+                        q_remove<true>(cand, (int)mi2, lane);
+                        if (lane < limit) first2 = __ldg(arow2 + lane);
+                        tr.expanded_nodes += 1;
+                        nrows = 2;
+                    }
+                }
+            }
             if constexpr (LM == 1 || LM == 2) {  // learned-stop checkpoint
-                ss.hops_kth += 1;
-                ss.hops_best += 1;
+                ss.hops_kth += nrows;
+                ss.hops_best += nrows;
                 const int t = tr.expanded_nodes;
                 // A checkpoint right after the k-th distance improved (hops_kth == 0 after the
                 // increment below is impossible; 1 means "improved by the last expansion")
@@ -1222,7 +1241,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 const bool want = LM == 1 || (a.stop_w != nullptr && a.stop_thr < INFINITY &&
                                               t >= a.min_expansions && ss.kth < INFINITY &&
                                               ss.hops_kth > 1);
-                if (t % a.ckpt_every == 0) {
+                if (t % a.ckpt_every < nrows) {  // a multiple of ckpt_every was reached
                     if (want) {
                         int c1 = 0, c11 = 0, c125 = 0;
                         const float k1 = ss.kth, k11 = ss.kth * 1.1f, k125 = ss.kth * 1.25f;
@@ -1270,6 +1289,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 }
             }
         }
+        for (int rr = 0; rr < nrows; ++rr)
         for (int c0 = 0; c0 < limit; c0 += 32) {
             const int j = c0 + lane;
             int nb = -1;
@@ -1278,8 +1298,10 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     nb = (given_seeds || (LM > 0 && seed_id >= 0)) ? seed_id
                                                   : (int)((unsigned long long)j * (unsigned long long)a.n /
                                                           (unsigned long long)a.n_multiprobe);
-                } else {
+                } else if (rr == 0) {
                     nb = c0 == 0 ? first : __ldg(arow + j);
+                } else {
+                    nb = c0 == 0 ? first2 : __ldg(arow2 + j);
                 }
             }
             if (nb >= a.n) {  // impossible for a validated graph; never read out of range

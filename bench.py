@@ -355,9 +355,9 @@ def run_ours(args, ws, rank, local):
             torch.cuda.synchronize()
             learn_s += time.time() - tl0
             blobs[tef] = song.get_model(g)
-            for lef in LEARN_SWEEP_EFS[tef]:
-                for thr in LEARN_THRESHOLDS:
-                    opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr)
+            for lef, thr, beam in [(e, t, b) for e in LEARN_SWEEP_EFS[tef] for t in LEARN_THRESHOLDS
+                                   for b in (1, 2)]:
+                    opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam)
                     song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
                     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                     e0.record(stream)
@@ -367,7 +367,8 @@ def run_ours(args, ws, rank, local):
                     ms = e0.elapsed_time(e1)
                     rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
                     trl = d_tr.cpu().numpy()
-                    pt = {"ef": lef, "trained_ef": tef, "threshold": thr, "recall": round(rec, 4),
+                    pt = {"ef": lef, "trained_ef": tef, "threshold": thr, "beam": beam,
+                          "recall": round(rec, 4),
                           "qps": round(NQ / ms * 1e3),
                           "mean_expanded": round(float(trl[:, 2].mean()), 1),
                           "mean_distance_evals": round(float(trl[:, 5].mean()), 1),
@@ -380,7 +381,8 @@ def run_ours(args, ws, rank, local):
             song.set_model(g, blobs[lbest["trained_ef"]])
             rep = reps[lbest["trained_ef"]]
             lprec = prec
-            lopts = song.SearchOpts(precision=lprec, learned=True, stop_threshold=lbest["threshold"])
+            lopts = song.SearchOpts(precision=lprec, learned=True, stop_threshold=lbest["threshold"],
+                                    beam=lbest["beam"])
             n0 = song.launch_count()
             lms, lkern, _ = timed_device(
                 torch, dist, ws, dev, stream, args.steps, args.warmup,
@@ -406,7 +408,8 @@ def run_ours(args, ws, rank, local):
             learned = {
                 "form": "tensor-core entry stage (4096 hubs) + learned entry/stop model, byte rows",
                 "precision": "u8 rows (exact for these integer vectors)" if row_bytes < DIM * 4 else "fp32",
-                "threshold": lbest["threshold"], "ef": lef, "trained_ef": lbest["trained_ef"],
+                "threshold": lbest["threshold"], "beam": lbest["beam"], "ef": lef,
+                "trained_ef": lbest["trained_ef"],
                 "qps": round(ws * NQ * args.steps / (lms / 1e3), 1),
                 "e2e_qps": round(ws * NQ * args.steps / l_e2e_s, 1),
                 "recall_at_10": round(float(ds.recall_at_k(ids_l, gt, K).mean()), 4),

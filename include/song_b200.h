@@ -98,7 +98,10 @@ typedef struct song_search_opts {
     int rerank;           /* 1: re-rank the final results queue with exact FP32 distances */
     int learned;          /* 1: use the index's learned entry/stop model                 */
     float stop_threshold; /* learned stop: stop when P(converged) >= threshold           */
-    int reserved[4];
+    int beam;             /* learned search: 2 = expand the two best candidates per step
+                             (both adjacency rows in one round trip; BLOCK_SIZE <= 32);
+                             0 or 1 = one per step, the reference's order              */
+    int reserved[3];
 } song_search_opts;
 
 /* Reference defaults of config.h:9-58. */

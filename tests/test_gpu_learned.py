@@ -95,3 +95,26 @@ def test_entry_stage_cuts_work_at_equal_recall(cuda, song, ds):
     assert rec_l >= rec_p - 0.01, (rec_p, rec_l)
     assert tl.queries[:, 5].mean() < 0.6 * tp.queries[:, 5].mean()
     g.close()
+
+
+def test_beam_two_expands_pairs(cuda, song, ds):
+    """Beam 2 expands the two best candidates per step: same recall within
+    0.01, and the search ends in fewer steps (expansions counted singly)."""
+    m, g, gt, rep = _setup(song, ds, n=30000, nq=400, ntrain=2000)
+    nq = m.queries.shape[0]
+    t1, t2 = song.GpuSearchTrace(), song.GpuSearchTrace()
+    ids1, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0),
+                                 m.queries, nq, 10, 64, trace=t1)
+    ids2, d2 = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0, beam=2),
+                                  m.queries, nq, 10, 64, trace=t2)
+    r1 = ds.recall_at_k(ids1, gt, 10).mean()
+    r2 = ds.recall_at_k(ids2, gt, 10).mean()
+    assert r2 >= r1 - 0.01, (r1, r2)
+    assert ((ids2 >= 0) & (ids2 < g.num_nodes)).all()
+    assert (np.diff(d2, axis=1) >= 0).all()          # best-first
+    assert t2.queries[:, 2].mean() > 0.8 * t1.queries[:, 2].mean()
+    # with a stop model too: checkpoints are still reached in steps of two
+    ids3, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=0.8, beam=2),
+                                 m.queries, nq, 10, 128)
+    assert ds.recall_at_k(ids3, gt, 10).mean() >= r1 - 0.05
+    g.close()
