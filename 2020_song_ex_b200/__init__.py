@@ -180,6 +180,10 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_bithash_project_device.argtypes = [vp, ci, ci, vp, i64, i64, vp, i64, vp]
     for name in ("song_bithash_matrix", "song_bithash_project", "song_bithash_project_device"):
         getattr(L, name).restype = C.c_int
+    L.song_exact_knn_device.argtypes = [vp, i64, i64, ci, vp, ci, i64, ci, vp, vp, vp]
+    L.song_exact_knn_device.restype = C.c_int
+    L.song_exact_knn.argtypes = [vp, i64, ci, vp, ci, ci, vp, vp]
+    L.song_exact_knn.restype = C.c_int
     for name in ("song_server_create", "song_server_submit", "song_server_poll",
                  "song_server_run_poisson", "song_server_destroy"):
         getattr(L, name).restype = C.c_int
@@ -495,6 +499,30 @@ def graph_search(g: KernelGraph, queries, nq: int, k: int, ef_search: int = 0):
     _check(load_library().song_graph_search(g._h, q.ctypes.data, nq, k, ef_search,
                                             ids.ctypes.data, tr.ctypes.data))
     return ids, tr
+
+
+def exact_knn_device(d_base, n: int, dim: int, d_queries, nq: int, k: int, d_ids, d_dists,
+                     ldb: Optional[int] = None, ldq: Optional[int] = None, stream=None) -> None:
+    """Exact kNN (squared L2) of device rows on the tensor cores: ids [nq, k]
+    int32 ascending by (distance, id) and their FP32 distances.  Replaces the
+    reference's brute force (bench_cpu.cpp:158-175, run_compare.py:199-213)."""
+    def ptr(t):
+        return C.c_void_p(t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+    st = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+    _check(load_library().song_exact_knn_device(
+        ptr(d_base), int(n), int(ldb if ldb is not None else dim), int(dim), ptr(d_queries),
+        int(nq), int(ldq if ldq is not None else dim), int(k), ptr(d_ids), ptr(d_dists), st))
+
+
+def exact_knn(base, queries, k: int):
+    """exact_knn_device on host arrays: returns (ids [nq, k] int32, dists [nq, k] f32)."""
+    b = np.ascontiguousarray(np.asarray(base, np.float32))
+    q = np.ascontiguousarray(np.asarray(queries, np.float32).reshape(-1, b.shape[1]))
+    ids = np.empty((q.shape[0], k), np.int32)
+    d = np.empty((q.shape[0], k), np.float32)
+    _check(load_library().song_exact_knn(b.ctypes.data, b.shape[0], b.shape[1], q.ctypes.data,
+                                         q.shape[0], int(k), ids.ctypes.data, d.ctypes.data))
+    return ids, d
 
 
 ENTRY_K = 24  # entry candidates per query (the entry model's inputs)

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsong_b200.so")
 SOURCES = ["song_search.cu", "song_build.cu", "song_learn.cu", "song_capi.cu", "song_serve.cu",
            "song_noalloc.cu", "song_bithash.cu", "song_entry.cu",
-           "song_graphsearch.cu"]
+           "song_graphsearch.cu", "song_gt.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

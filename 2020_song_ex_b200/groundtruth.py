@@ -1,15 +1,18 @@
 """Exact k-nearest-neighbour ground truth on the GPU, for recall.
 
 The reference computes ground truth by sequential brute force on the CPU
-(bench_cpu.cpp:158-175) or in numpy (run_compare.py:199-213).  Here
-``||q - b||^2 = ||q||^2 - 2 q.b + ||b||^2`` with the cross term from
-tensor-core GEMMs on 3xBF16 split operands: x = hi + lo with hi = bf16(x)
-and lo = bf16(x - hi), and q.b ~= hi_q.hi_b + hi_q.lo_b + lo_q.hi_b with FP32
-accumulation (the lo.lo term is below FP32 resolution).  For integer data in
-[0, 255] (the SIFT-shaped workloads) lo is exactly zero and every sum is an
-integer below 2^24, so the distances are exact.  ``spot_check`` recomputes a
-sample of queries in FP64 and reports how many true top-k ids the GPU
-ground truth misses.
+(bench_cpu.cpp:158-175) or in numpy (run_compare.py:199-213).  ``knn`` runs
+the library's tensor-core kernel (``song_exact_knn_device``):
+``||q - b||^2 = ||q||^2 - 2 q.b + ||b||^2`` with the cross term from 3xBF16
+split operands, x = hi + lo with hi = bf16(x) and lo = bf16(x - hi), and
+q.b ~= hi_q.hi_b + hi_q.lo_b + lo_q.hi_b accumulated in FP32 (the lo.lo term
+is below FP32 resolution), the k smallest kept per query in the kernel's
+epilogue, ties broken by the lower id.  For integer data in [0, 255] (the
+SIFT-shaped workloads) lo is exactly zero and every sum is an integer below
+2^24, so the distances are exact.  ``knn_torch`` computes the same split
+products with library GEMMs (a cross-check for tests).  ``spot_check``
+recomputes a sample of queries in FP64 and reports how many true top-k ids
+the GPU ground truth misses.
 """
 from __future__ import annotations
 
@@ -29,8 +32,24 @@ def _mm(a, b):
     return torch.mm(a, b, out_dtype=torch.float32)
 
 
-def knn(base, queries, k: int, chunk: int = 2048, device: str = "cuda"):
-    """Exact top-k ids [nq, k] (ascending distance) and their FP32 distances."""
+def knn(base, queries, k: int, device: str = "cuda"):
+    """Exact top-k ids [nq, k] int32 (ascending (distance, id)) and their FP32
+    distances, from the tensor-core kernel."""
+    import torch
+    from . import exact_knn_device
+    b = torch.as_tensor(np.ascontiguousarray(base, dtype=np.float32), device=device)
+    q = torch.as_tensor(np.ascontiguousarray(queries, dtype=np.float32), device=device)
+    q = q.reshape(-1, b.shape[1])
+    ids = torch.empty((q.shape[0], k), dtype=torch.int32, device=device)
+    dists = torch.empty((q.shape[0], k), dtype=torch.float32, device=device)
+    exact_knn_device(b, b.shape[0], b.shape[1], q, q.shape[0], k, ids, dists,
+                     stream=torch.cuda.current_stream())
+    return ids.cpu().numpy(), dists.cpu().numpy()
+
+
+def knn_torch(base, queries, k: int, chunk: int = 2048, device: str = "cuda"):
+    """The same split products with library GEMMs and torch.topk (ties in
+    arbitrary order): top-k ids [nq, k] and FP32 distances."""
     import torch
     b = torch.as_tensor(np.ascontiguousarray(base, dtype=np.float32), device=device)
     q_all = torch.as_tensor(np.ascontiguousarray(queries, dtype=np.float32), device=device)

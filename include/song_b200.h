@@ -249,6 +249,23 @@ song_status song_bithash_project_device(const float* d_R, int dim, int hash_bits
                                         uint32_t* d_codes, int64_t ldc, void* stream);
 
 /*
+ * Exact k nearest neighbours by squared L2 (the ground truth recall is
+ * measured against).  Replaces the reference's brute force
+ * (bench_cpu.cpp:158-175, main.cpp:14-49; numpy in run_compare.py:199-213).
+ * Distances are |q|^2 - 2 q.b + |b|^2 with the cross term from 3xBF16
+ * split products on the tensor cores (FP32 accumulation; exact for integer
+ * data in [0, 255] with dim <= 128).  Output per query: k ids ascending by
+ * (distance, id), -1 / +inf when n < k.  1 <= k <= 128.
+ * The device form takes device buffers (row strides ldb, ldq in floats) and
+ * returns when the result is on the device (it synchronises `stream`).
+ */
+song_status song_exact_knn_device(const float* d_base, int64_t n, int64_t ldb, int dim,
+                                  const float* d_queries, int nq, int64_t ldq, int k,
+                                  int32_t* d_ids, float* d_dists, void* stream);
+song_status song_exact_knn(const float* base, int64_t n, int dim, const float* queries, int nq,
+                           int k, int32_t* ids, float* dists);
+
+/*
  * Attach a compressed copy of an L2 index's vectors for the precision form
  * (SONG_PREC_BF16 or SONG_PREC_FP8), converted on the GPU from the FP32
  * copy, which stays resident for the exact re-rank.  Replaces an earlier
