@@ -70,7 +70,8 @@ class _Timing(C.Structure):
 
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("rerank", C.c_int), ("learned", C.c_int),
-                ("stop_threshold", C.c_float), ("beam", C.c_int), ("reserved", C.c_int * 3)]
+                ("stop_threshold", C.c_float), ("beam", C.c_int), ("bloom_hashes", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 @dataclass
@@ -82,10 +83,11 @@ class SearchOpts:
     learned: bool = False
     stop_threshold: float = 0.5
     beam: int = 1  # learned search: 2 expands the two best candidates per step
+    bloom_hashes: int = 0  # learned search: Bloom hashes per id (0 = the index's bf_nhash)
 
     def _c(self) -> _Opts:
         return _Opts(int(self.precision), int(bool(self.rerank)), int(bool(self.learned)),
-                     float(self.stop_threshold), int(self.beam))
+                     float(self.stop_threshold), int(self.beam), int(self.bloom_hashes))
 
 
 class _LearnParams(C.Structure):

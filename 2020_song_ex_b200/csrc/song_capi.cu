@@ -353,6 +353,8 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
         a->qdim = song::lowp_padded_dim(prec, x->dim);
         a->rerank = opts->rerank ? 1 : 0;
     }
+    if (opts && !opts->learned && opts->bloom_hashes != 0)
+        return fail(SONG_ERR_INVALID_ARG, "bloom_hashes applies to learned searches only");
     if (opts && opts->learned) {
         if (!x->has_model) return fail(SONG_ERR_INVALID_ARG, "no learned model attached (song_index_learn)");
         if (x->kind != SONG_KIND_L2 || cap > 1024)
@@ -365,6 +367,11 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
         a->ckpt_every = x->ckpt_every;
         a->min_expansions = x->min_expansions;
         a->beam = opts->beam >= 2 ? 2 : 1;
+        if (opts->bloom_hashes != 0) {
+            if (opts->bloom_hashes < 1 || opts->bloom_hashes > 4)
+                return fail(SONG_ERR_INVALID_ARG, "bloom_hashes must be 0 or in [1, 4]");
+            a->bf_nhash = opts->bloom_hashes;
+        }
         const float t = opts->stop_threshold;
         a->stop_thr = t <= 0.0f ? -INFINITY : (t >= 1.0f ? INFINITY : std::log(t / (1.0f - t)));
     }

@@ -84,6 +84,16 @@ __device__ __forceinline__ unsigned tm_ld(uint32_t taddr) {
         : "memory");
     return r;
 }
+// Two columns with one wait.
+__device__ __forceinline__ void tm_ld2(uint32_t a0, uint32_t a1, unsigned& r0, unsigned& r1) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%2];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%1}, [%3];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r0), "=r"(r1)
+        : "r"(a0), "r"(a1)
+        : "memory");
+}
 __device__ __forceinline__ void tm_st(uint32_t taddr, unsigned v) {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};\n\t"
@@ -225,6 +235,41 @@ __device__ __forceinline__ void q_remove(Queue<GPL, TM>& q, int hole, int lane) 
     q.sz = last;
     group_update<MIN>(q, hole >> 5, lane);
     if ((last >> 5) != (hole >> 5)) group_update<MIN>(q, last >> 5, lane);
+}
+
+// Id of slot `hole`, then q_remove(hole): the same queue afterwards, with the
+// TMEM columns of `hole` and of the last slot read once (one wait) instead
+// of once per id access.
+template <bool MIN, int GPL, int TM>
+__device__ __forceinline__ int q_pop(Queue<GPL, TM>& q, int hole, int lane) {
+    if constexpr (!TM) {
+        const int id = q.id[hole];
+        q_remove<MIN>(q, hole, lane);
+        return id;
+    } else {
+        const int last = q.sz - 1;
+        const uint32_t ch = q.tid + (uint32_t)(hole >> 5), cl = q.tid + (uint32_t)(last >> 5);
+        unsigned rh, rl;
+        if (ch == cl) {
+            rh = tm_ld(ch);
+            rl = rh;
+        } else {
+            tm_ld2(ch, cl, rh, rl);
+        }
+        const int id = (int)__shfl_sync(FULL, rh, hole & 31);
+        const unsigned idl = __shfl_sync(FULL, rl, last & 31);
+        __syncwarp();
+        if (hole != last) {
+            if (lane == 0) q.d[hole] = q.d[last];
+            if (lane == (hole & 31)) rh = idl;
+            tm_st(ch, rh);
+        }
+        __syncwarp();
+        q.sz = last;
+        group_update<MIN>(q, hole >> 5, lane);
+        if ((last >> 5) != (hole >> 5)) group_update<MIN>(q, last >> 5, lane);
+        return id;
+    }
 }
 
 // Push (d, nb) of every lane in N, in lane order, with the semantics of
@@ -1200,10 +1245,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             unsigned mb, mi;
             root_min(cand, mb, mi);
             const float cmin = __uint_as_float(mb);
-            const int cn = q_id(cand, (int)mi);
+            const int cn = q_pop<true>(cand, (int)mi, lane);
             limit = a.block_size;
             arow = a.adj + (int64_t)cn * a.block_size;
-            q_remove<true>(cand, (int)mi, lane);
             if (lane < limit) first = __ldg(arow + lane);
             tr.expanded_nodes += 1;
             unsigned wb = 0xffffffffu, wi;
@@ -1222,9 +1266,8 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     unsigned mb2, mi2;
                     root_min(cand, mb2, mi2);
                     if (!(res.sz == res.cap && mb2 > wb)) {
-                        const int cn2 = q_id(cand, (int)mi2);
+                        const int cn2 = q_pop<true>(cand, (int)mi2, lane);
                         arow2 = a.adj + (int64_t)cn2 * a.block_size;
-                        q_remove<true>(cand, (int)mi2, lane);
                         if (lane < limit) first2 = __ldg(arow2 + lane);
                         tr.expanded_nodes += 1;
                         nrows = 2;

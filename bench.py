@@ -56,6 +56,7 @@ BF_SWEEP = (256, 512, 1024)
 LEARN_THRESHOLDS = (0.8, 0.9, 0.95, 0.98, 1.0)   # 1.0: entry stage alone, no learned stop
 LEARN_EFS = (96, 160)                              # queue sizes the models are trained at
 LEARN_SWEEP_EFS = {96: (64, 96, 128), 160: (160, 192, 256)}
+LEARN_BLOOM_HASHES = (4, 2)                        # BF_NHASH, and the learned search's cheaper test
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
 
 
@@ -355,20 +356,25 @@ def run_ours(args, ws, rank, local):
             torch.cuda.synchronize()
             learn_s += time.time() - tl0
             blobs[tef] = song.get_model(g)
-            for lef, thr, beam in [(e, t, b) for e in LEARN_SWEEP_EFS[tef] for t in LEARN_THRESHOLDS
-                                   for b in (1, 2)]:
-                    opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam)
+            for lef, thr, beam, nh in [(e, t, b, h) for e in LEARN_SWEEP_EFS[tef]
+                                       for t in LEARN_THRESHOLDS for b in (1, 2)
+                                       for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))]:
+                    opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam,
+                                           bloom_hashes=nh)
                     song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    e0.record(stream)
-                    song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, None, stream=stream)
-                    e1.record(stream)
-                    stream.synchronize()
-                    ms = e0.elapsed_time(e1)
                     rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
                     trl = d_tr.cpu().numpy()
+                    mss = []
+                    for _ in range(3):  # median of three launches
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, None, stream=stream)
+                        e1.record(stream)
+                        stream.synchronize()
+                        mss.append(e0.elapsed_time(e1))
+                    ms = statistics.median(mss)
                     pt = {"ef": lef, "trained_ef": tef, "threshold": thr, "beam": beam,
-                          "recall": round(rec, 4),
+                          "bloom_hashes": nh, "recall": round(rec, 4),
                           "qps": round(NQ / ms * 1e3),
                           "mean_expanded": round(float(trl[:, 2].mean()), 1),
                           "mean_distance_evals": round(float(trl[:, 5].mean()), 1),
@@ -382,7 +388,7 @@ def run_ours(args, ws, rank, local):
             rep = reps[lbest["trained_ef"]]
             lprec = prec
             lopts = song.SearchOpts(precision=lprec, learned=True, stop_threshold=lbest["threshold"],
-                                    beam=lbest["beam"])
+                                    beam=lbest["beam"], bloom_hashes=lbest["bloom_hashes"])
             n0 = song.launch_count()
             lms, lkern, _ = timed_device(
                 torch, dist, ws, dev, stream, args.steps, args.warmup,
@@ -408,7 +414,8 @@ def run_ours(args, ws, rank, local):
             learned = {
                 "form": "tensor-core entry stage (4096 hubs) + learned entry/stop model, byte rows",
                 "precision": "u8 rows (exact for these integer vectors)" if row_bytes < DIM * 4 else "fp32",
-                "threshold": lbest["threshold"], "beam": lbest["beam"], "ef": lef,
+                "threshold": lbest["threshold"], "beam": lbest["beam"],
+                "bloom_hashes": lbest["bloom_hashes"], "ef": lef,
                 "trained_ef": lbest["trained_ef"],
                 "qps": round(ws * NQ * args.steps / (lms / 1e3), 1),
                 "e2e_qps": round(ws * NQ * args.steps / l_e2e_s, 1),
@@ -481,7 +488,9 @@ def run_ours(args, ws, rank, local):
             "config": {
                 "workload": WORKLOAD, "n": N_BASE, "dim": DIM, "nq_per_gpu": NQ, "k": K,
                 "form": "learned" if use_learned else "plain",
-                "ef": ef, "bf_words": best["bf_words"], "pq_size": 1024,
+                "ef": learned["ef"] if use_learned else ef, "bf_words": best["bf_words"],
+                "bloom_hashes": learned["bloom_hashes"] if use_learned else 4,
+                "beam": learned["beam"] if use_learned else 1, "pq_size": 1024,
                 "graph": "GPU batched-insertion NSW (ratio 32)",
                 "l2": "inputs larger than L2 (data 512 MB + adj 128 MB per GPU)",
                 "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",

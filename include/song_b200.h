@@ -101,7 +101,10 @@ typedef struct song_search_opts {
     int beam;             /* learned search: 2 = expand the two best candidates per step
                              (both adjacency rows in one round trip; BLOCK_SIZE <= 32);
                              0 or 1 = one per step, the reference's order              */
-    int reserved[3];
+    int bloom_hashes;     /* learned search: Bloom hashes per id (1..4) in place of the
+                             index's bf_nhash (BF_NHASH); 0 = the index's value.  Plain
+                             searches reject it: they keep the reference's visited set */
+    int reserved[2];
 } song_search_opts;
 
 /* Reference defaults of config.h:9-58. */

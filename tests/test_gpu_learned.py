@@ -118,3 +118,30 @@ def test_beam_two_expands_pairs(cuda, song, ds):
                                  m.queries, nq, 10, 128)
     assert ds.recall_at_k(ids3, gt, 10).mean() >= r1 - 0.05
     g.close()
+
+
+def test_bloom_hashes_option(cuda, song, ds):
+    """A learned search may test visited ids with fewer Bloom hashes than the
+    index's BF_NHASH (a cheaper test, a few more false 'visited'): recall stays
+    within 0.01 (0.02 with one hash) and the output stays valid; the default (0) is the index's
+    value, bit for bit; a plain search refuses the option, so it keeps the
+    reference's visited set."""
+    m, g, gt, rep = _setup(song, ds, n=30000, nq=400, ntrain=2000)
+    nq = m.queries.shape[0]
+    o4 = song.SearchOpts(learned=True, stop_threshold=1.0)
+    ids4, _ = song.gpu_search_ex(g, o4, m.queries, nq, 10, 64)
+    ids4b, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0,
+                                                     bloom_hashes=4), m.queries, nq, 10, 64)
+    np.testing.assert_array_equal(ids4, ids4b)
+    for nh in (1, 2, 3):
+        ids, d = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0,
+                                                       bloom_hashes=nh), m.queries, nq, 10, 64)
+        assert ((ids >= 0) & (ids < g.num_nodes)).all()
+        assert (np.diff(d, axis=1) >= 0).all()
+        tol = 0.02 if nh == 1 else 0.01
+        assert ds.recall_at_k(ids, gt, 10).mean() >= ds.recall_at_k(ids4, gt, 10).mean() - tol
+    with pytest.raises(song.SongError):
+        song.gpu_search_ex(g, song.SearchOpts(learned=True, bloom_hashes=5), m.queries, nq, 10, 64)
+    with pytest.raises(song.SongError):
+        song.gpu_search_ex(g, song.SearchOpts(bloom_hashes=2), m.queries, nq, 10, 64)
+    g.close()
