@@ -1322,7 +1322,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     ss.n_new = ss.n_res = ss.n_front = 0;
                 }
             }
-            if (cand.sz > 0) {  // the next pop is most often today's runner-up: warm its row in L2
+            // The next pop is most often today's runner-up: warm its row in L2.  Learned
+            // searches (short queues, rows mostly L2-resident) measured faster without it.
+            if (LM == 0 && cand.sz > 0) {
                 unsigned nb2, ni2;
                 root_min(cand, nb2, ni2);
                 const int nid = q_id(cand, (int)ni2);

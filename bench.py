@@ -51,11 +51,11 @@ K = 10
 SEED = 2020
 BLOCK_SIZE = 32
 TARGET_RECALL = 0.95
-EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 512, 640, 768, 1024)
+EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 480, 512, 640, 768, 1024)
 BF_SWEEP = (256, 512, 1024)
 LEARN_THRESHOLDS = (0.8, 0.9, 0.95, 0.98, 1.0)   # 1.0: entry stage alone, no learned stop
 LEARN_EFS = (96, 160)                              # queue sizes the models are trained at
-LEARN_SWEEP_EFS = {96: (64, 96, 128), 160: (160, 192, 256)}
+LEARN_SWEEP_EFS = {96: (64, 80, 88, 96, 128), 160: (160, 192, 256)}
 LEARN_BLOOM_HASHES = (4, 2)                        # BF_NHASH, and the learned search's cheaper test
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
 
