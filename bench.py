@@ -185,10 +185,12 @@ def _gpu_index(local: int) -> int:
     return local
 
 
-def timed_device(torch, dist, ws, dev, stream, steps, warmup, launch, clocks_gpu=None):
+def timed_device(torch, dist, ws, dev, stream, steps, warmup, launch, clocks_gpu=None, count=None):
     """Warm up, then time `steps` launches on `stream` with CUDA events
     (barrier + synchronize on both sides, max over ranks).  Returns
-    (total_ms, per-step kernel ms list, clock summary or None)."""
+    (total_ms, per-step kernel ms list, clock summary or None).  With
+    `count` (the library's launch counter), timed_device.last_launches is the
+    number of kernels launched inside the timed loop."""
     for _ in range(warmup):
         launch()
     stream.synchronize()
@@ -203,12 +205,14 @@ def timed_device(torch, dist, ws, dev, stream, steps, warmup, launch, clocks_gpu
         clk.__enter__()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    n_before = count() if count is not None else 0
     t_start.record(stream)
     for i in range(steps):
         evs[i][0].record(stream)
         launch()
         evs[i][1].record(stream)
     t_end.record(stream)
+    timed_device.last_launches = (count() - n_before) if count is not None else None
     stream.synchronize()
     torch.cuda.synchronize()
     if clk:
@@ -311,12 +315,11 @@ def run_ours(args, ws, rank, local):
                                      bf_words=best["bf_words"])
         parity = bool((oids == ids_op[:sample]).all() and (otr == trace[:sample]).all())
 
-    n0 = song.launch_count()
     plain_ms, plain_kern, clocks = timed_device(
         torch, dist, ws, dev, stream, args.steps, args.warmup,
         lambda: song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream),
-        clocks_gpu=_gpu_index(local))
-    plain_launches = song.launch_count() - n0
+        clocks_gpu=_gpu_index(local), count=song.launch_count)
+    plain_launches = timed_device.last_launches
     plain_qps = ws * NQ * args.steps / (plain_ms / 1e3)
     if args.no_e2e:
         g.close()
@@ -362,6 +365,7 @@ def run_ours(args, ws, rank, local):
                     opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam,
                                            bloom_hashes=nh)
                     song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
+                    stream.synchronize()  # the ids and traces of this point, not the previous one
                     rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
                     trl = d_tr.cpu().numpy()
                     mss = []
@@ -389,12 +393,11 @@ def run_ours(args, ws, rank, local):
             lprec = prec
             lopts = song.SearchOpts(precision=lprec, learned=True, stop_threshold=lbest["threshold"],
                                     beam=lbest["beam"], bloom_hashes=lbest["bloom_hashes"])
-            n0 = song.launch_count()
             lms, lkern, _ = timed_device(
                 torch, dist, ws, dev, stream, args.steps, args.warmup,
                 lambda: song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, None,
-                                              stream=stream))
-            l_launches = song.launch_count() - n0
+                                              stream=stream), count=song.launch_count)
+            l_launches = timed_device.last_launches
             ids_l = d_ids.cpu().numpy()
             song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
             stream.synchronize()

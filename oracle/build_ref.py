@@ -80,6 +80,7 @@ DEFAULT_VARIANTS = [
     RefVariant(),
     # the benchmark's operating points (queue cap 1024)
     RefVariant(pq_size=1024, bf_words=256),
+    RefVariant(pq_size=1024, bf_words=512),
     RefVariant(pq_size=1024, bf_words=1024),
 ]
 
