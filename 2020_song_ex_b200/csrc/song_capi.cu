@@ -366,7 +366,7 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
         a->stop_w = x->d_stop_w;
         a->ckpt_every = x->ckpt_every;
         a->min_expansions = x->min_expansions;
-        a->beam = opts->beam >= 2 ? 2 : 1;
+        a->beam = opts->beam < 1 ? 1 : (opts->beam > 4 ? 4 : opts->beam);
         if (opts->bloom_hashes != 0) {
             if (opts->bloom_hashes < 1 || opts->bloom_hashes > 4)
                 return fail(SONG_ERR_INVALID_ARG, "bloom_hashes must be 0 or in [1, 4]");

@@ -57,7 +57,7 @@ struct SearchArgs {
     int n_hubs;
     const __half* entry_w;   // packed entry MLP (kFeat -> kHid -> kHid -> n_hubs), nullable
     const __half* stop_w;    // packed stop MLP (kFeat -> kHid -> kHid -> 1), nullable
-    int beam;                // learned searches: candidates expanded per step (1 or 2)
+    int beam;                // learned searches: candidates expanded per step (1 to 4)
     int ckpt_every;          // expansions between stop checkpoints
     int min_expansions;      // no learned stop before this many expansions
     float stop_thr;          // stop when sigmoid(stop logit) >= stop_thr

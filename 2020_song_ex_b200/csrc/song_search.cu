@@ -1235,8 +1235,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     for (;;) {
         int limit;
         const int32_t* arow = nullptr;
-        const int32_t* arow2 = nullptr;  // learned search, beam 2: a second row this step
-        int first = -1, first2 = -1;      // first chunk of each adjacency row
+        // first chunk of each adjacency row; learned searches with beam > 1 expand up
+        // to 3 more rows this step (BLOCK_SIZE <= 32: one chunk per row)
+        int first = -1, first2 = -1, first3 = -1, first4 = -1;
         int nrows = 1;
         if (seeding) {
             limit = n_seeds;  // seeds p*n/N_MULTIPROBE (kernalGraph.h:214-231)
@@ -1259,18 +1260,21 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 }
             }
             if constexpr (LM > 0) {
-                // Beam 2 (learned searches only; not the reference's order): the
-                // runner-up is expanded in the same step when it would not end the
-                // search, so both adjacency rows are fetched in one round trip.
-                if (a.beam > 1 && cand.sz > 0 && a.block_size <= 32) {
-                    unsigned mb2, mi2;
-                    root_min(cand, mb2, mi2);
-                    if (!(res.sz == res.cap && mb2 > wb)) {
+                // Beam (learned searches only; not the reference's order): the next
+                // best candidates are expanded in the same step while they would not
+                // end the search, so their adjacency rows are fetched in one round trip.
+                if (a.beam > 1 && a.block_size <= 32) {
+                    for (int bb = 1; bb < a.beam && cand.sz > 0; ++bb) {
+                        unsigned mb2, mi2;
+                        root_min(cand, mb2, mi2);
+                        if (res.sz == res.cap && mb2 > wb) break;
                         const int cn2 = q_pop<true>(cand, (int)mi2, lane);
-                        arow2 = a.adj + (int64_t)cn2 * a.block_size;
-                        if (lane < limit) first2 = __ldg(arow2 + lane);
+                        const int f = lane < limit ? __ldg(a.adj + (int64_t)cn2 * a.block_size + lane) : -1;
+                        if (bb == 1) first2 = f;
+                        else if (bb == 2) first3 = f;
+                        else first4 = f;
                         tr.expanded_nodes += 1;
-                        nrows = 2;
+                        nrows = bb + 1;
                     }
                 }
             }
@@ -1345,8 +1349,8 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                                                           (unsigned long long)a.n_multiprobe);
                 } else if (rr == 0) {
                     nb = c0 == 0 ? first : __ldg(arow + j);
-                } else {
-                    nb = c0 == 0 ? first2 : __ldg(arow2 + j);
+                } else {  // beam rows: one chunk each
+                    nb = rr == 1 ? first2 : (rr == 2 ? first3 : first4);
                 }
             }
             if (nb >= a.n) {  // impossible for a validated graph; never read out of range

@@ -55,7 +55,8 @@ EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 480, 512, 640, 768, 1024)
 BF_SWEEP = (256, 512, 1024)
 LEARN_THRESHOLDS = (0.8, 0.9, 0.95, 0.98, 1.0)   # 1.0: entry stage alone, no learned stop
 LEARN_EFS = (96, 160)                              # queue sizes the models are trained at
-LEARN_SWEEP_EFS = {96: (64, 80, 88, 96, 128), 160: (160, 192, 256)}
+LEARN_SWEEP_EFS = {96: (64, 72, 80, 88, 96, 128), 160: (160, 192, 256)}
+LEARN_BEAMS = (1, 2, 3, 4)                         # candidates expanded per step
 LEARN_BLOOM_HASHES = (4, 2)                        # BF_NHASH, and the learned search's cheaper test
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
 
@@ -359,8 +360,11 @@ def run_ours(args, ws, rank, local):
             torch.cuda.synchronize()
             learn_s += time.time() - tl0
             blobs[tef] = song.get_model(g)
+            # threshold 1.0 (entry model only): every beam and Bloom hash count;
+            # learned stop: beam 1 and 2 with 2 hashes
             for lef, thr, beam, nh in [(e, t, b, h) for e in LEARN_SWEEP_EFS[tef]
-                                       for t in LEARN_THRESHOLDS for b in (1, 2)
+                                       for t in LEARN_THRESHOLDS
+                                       for b in (LEARN_BEAMS if t >= 1.0 else (1, 2))
                                        for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))]:
                     opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam,
                                            bloom_hashes=nh)

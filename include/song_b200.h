@@ -98,9 +98,10 @@ typedef struct song_search_opts {
     int rerank;           /* 1: re-rank the final results queue with exact FP32 distances */
     int learned;          /* 1: use the index's learned entry/stop model                 */
     float stop_threshold; /* learned stop: stop when P(converged) >= threshold           */
-    int beam;             /* learned search: 2 = expand the two best candidates per step
-                             (both adjacency rows in one round trip; BLOCK_SIZE <= 32);
-                             0 or 1 = one per step, the reference's order              */
+    int beam;             /* learned search: 2..4 = expand that many best candidates per
+                             step (their adjacency rows in one round trip; BLOCK_SIZE
+                             <= 32; values above 4 act as 4); 0 or 1 = one per step,
+                             the reference's order                                     */
     int bloom_hashes;     /* learned search: Bloom hashes per id (1..4) in place of the
                              index's bf_nhash (BF_NHASH); 0 = the index's value.  Plain
                              searches reject it: they keep the reference's visited set */

@@ -113,6 +113,13 @@ def test_beam_two_expands_pairs(cuda, song, ds):
     assert ((ids2 >= 0) & (ids2 < g.num_nodes)).all()
     assert (np.diff(d2, axis=1) >= 0).all()          # best-first
     assert t2.queries[:, 2].mean() > 0.8 * t1.queries[:, 2].mean()
+    # beams 3 and 4: valid best-first output, recall not below beam 1's
+    for beam in (3, 4):
+        ids_b, d_b = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0,
+                                                           beam=beam), m.queries, nq, 10, 64)
+        assert ((ids_b >= 0) & (ids_b < g.num_nodes)).all()
+        assert (np.diff(d_b, axis=1) >= 0).all()
+        assert ds.recall_at_k(ids_b, gt, 10).mean() >= r1 - 0.01
     # with a stop model too: checkpoints are still reached in steps of two
     ids3, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=0.8, beam=2),
                                  m.queries, nq, 10, 128)
