@@ -36,6 +36,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -81,7 +82,7 @@ class Clocks:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"song_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
