@@ -105,6 +105,7 @@ struct EntryArgs {
     float* out_d;              // [nq x kK]
     float* part_key;           // splits > 1: [splits x nq x kK] keys |h|^2 - 2 q.h
     int32_t* part_idx;         // splits > 1: [splits x nq x kK] hub indices (-1 = none)
+    int* tile_done;            // splits > 1: [query tiles] CTAs finished, zero at launch
     int* err;                  // set to 2 when a bounded wait gives up
 };
 
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     }
     if (!ok && tid == 0) atomicExch(a.err, 2);
     if (q < a.nq) {
-        if (gridDim.y > 1) {  // partial list of this split, merged by entry_merge
+        if (gridDim.y > 1) {  // partial list of this split, merged below by the tile's last CTA
             const size_t o = ((size_t)blockIdx.y * a.nq + q) * kK;
             for (int i = 0; i < kK; ++i) {
                 const bool v = ok && ki[i] >= 0 && kd[i] < INFINITY;
@@ -284,65 +285,50 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
             }
         }
     }
+    if (gridDim.y > 1) {
+        // The last CTA of this query tile to finish merges the splits' lists: per
+        // query the kK smallest (key, hub index), the order the unsplit kernel
+        // keeps.  Each list is sorted that way (sorted insertion, hubs visited in
+        // increasing index), so a merge of the list heads suffices.
+        __shared__ int is_last;
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) is_last = atomicAdd(a.tile_done + blockIdx.x, 1) == (int)gridDim.y - 1;
+        __syncthreads();
+        if (is_last) {
+            __threadfence();
+            if (q < a.nq) {
+                int pos[kEntrySplits];
+                const int S = (int)gridDim.y;
+                for (int sp = 0; sp < S; ++sp) pos[sp] = 0;
+                for (int i = 0; i < kK; ++i) {
+                    float bk = INFINITY;
+                    int bi = INT_MAX, bs = -1;
+                    for (int sp = 0; sp < S; ++sp) {
+                        if (pos[sp] >= kK) continue;
+                        const size_t o = ((size_t)sp * a.nq + q) * kK + pos[sp];
+                        const int idx = __ldcg(a.part_idx + o);
+                        if (idx < 0) continue;
+                        const float key = __ldcg(a.part_key + o);
+                        if (key < bk || (key == bk && idx < bi)) {
+                            bk = key;
+                            bi = idx;
+                            bs = sp;
+                        }
+                    }
+                    if (bs >= 0) ++pos[bs];
+                    a.out_ids[(size_t)q * kK + i] = bs >= 0 ? __ldg(a.hub_ids + bi) : -1;
+                    a.out_d[(size_t)q * kK + i] = bs >= 0 ? fmaxf(qn + bk, 0.0f) : INFINITY;
+                }
+            }
+        }
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kN)
                      : "memory");
-}
-
-// Merge of the splits' partial lists: one warp per query keeps the kK
-// smallest (key, hub index) -- the order the unsplit kernel keeps -- and
-// writes node ids and squared distances (|q|^2 from the FP32 query, as the
-// unsplit kernel adds it).
-__global__ void entry_merge(const float* __restrict__ part_key, const int32_t* __restrict__ part_idx,
-                            int splits, int nq, const float* __restrict__ queries, int qld, int dim,
-                            const int32_t* __restrict__ hub_ids, int32_t* __restrict__ out_ids,
-                            float* __restrict__ out_d) {
-    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (q >= nq) return;
-    float qn = 0.0f;
-    if (lane == 0)
-        for (int k = 0; k < dim; ++k) {
-            const float x = queries[(size_t)q * qld + k];
-            qn = fmaf(x, x, qn);
-        }
-    qn = __shfl_sync(0xffffffffu, qn, 0);
-    const int total = splits * kK;
-    for (int i = 0; i < kK; ++i) {  // i-th smallest (key, index) over all splits
-        float bk = INFINITY;
-        int bi = INT_MAX, bs = -1;
-        for (int c = lane; c < total; c += 32) {
-            const size_t o = ((size_t)(c / kK) * nq + q) * kK + (c % kK);
-            const int idx = part_idx[o];
-            const float key = part_key[o];
-            if (idx >= 0 && (key < bk || (key == bk && idx < bi))) {
-                bk = key;
-                bi = idx;
-                bs = (int)o;
-            }
-        }
-#pragma unroll
-        for (int w = 16; w >= 1; w >>= 1) {
-            const float ok2 = __shfl_xor_sync(0xffffffffu, bk, w);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, w);
-            const int os = __shfl_xor_sync(0xffffffffu, bs, w);
-            if (os >= 0 && (bs < 0 || ok2 < bk || (ok2 == bk && oi < bi))) {
-                bk = ok2;
-                bi = oi;
-                bs = os;
-            }
-        }
-        if (lane == 0) {
-            out_ids[(size_t)q * kK + i] = bs >= 0 ? __ldg(hub_ids + bi) : -1;
-            out_d[(size_t)q * kK + i] = bs >= 0 ? fmaxf(qn + bk, 0.0f) : INFINITY;
-        }
-        __syncwarp();
-        if (lane == 0 && bs >= 0) const_cast<int32_t*>(part_idx)[bs] = -1;  // taken
-        __syncwarp();
-    }
 }
 
 // Hub tiles from FP32 base rows: hub i of the set is node ids[i] (-1 =
@@ -407,11 +393,17 @@ size_t entry_smem_bytes(int dim) {
     return (size_t)kM * kp * 2 + 2 * (size_t)kN * kp * 2;
 }
 
+// Bytes of the per-tile arrival counters at the front of the split scratch.
+static size_t tile_done_bytes(int nq) {
+    const size_t qt = (size_t)(std::max(nq, 1) + kM - 1) / kM;
+    return (qt * 4 + 255) / 256 * 256;
+}
+
 size_t entry_split_scratch_bytes(int nq, int num_sms) {
     const int qt = (nq + kM - 1) / kM;
     int splits = qt <= 1 ? kEntrySplits : (2 * num_sms) / qt;
     splits = std::max(1, std::min(kEntrySplits, splits));
-    return (size_t)splits * std::max(nq, 1) * kK * 8;
+    return tile_done_bytes(nq) + (size_t)splits * std::max(nq, 1) * kK * 8;
 }
 
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
@@ -434,31 +426,32 @@ cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
     a.out_d = d_out_d;
     // The hub tiles are spread over `splits` CTAs per 128 queries (about two
     // CTAs per SM in all, up to kEntrySplits), as far as the caller's scratch
-    // holds their partial lists; the lists are merged afterwards.  The result
-    // does not depend on the split.
+    // holds their partial lists and the per-tile arrival counters; the last CTA
+    // of each query tile merges the lists.  The result does not depend on the
+    // split.
     const int qt = (nq + kM - 1) / kM;
     int splits = qt <= 1 ? kEntrySplits : (2 * num_sms) / qt;
     splits = std::max(1, std::min(std::min(kEntrySplits, a.ntiles), splits));
-    const size_t per_split = (size_t)nq * kK * 8;
-    if (split_scratch == nullptr) splits = 1;
-    else splits = (int)std::min<size_t>((size_t)splits, split_bytes / per_split);
+    const size_t per_split = (size_t)nq * kK * 8, head = tile_done_bytes(nq);
+    if (split_scratch == nullptr || split_bytes < head) splits = 1;
+    else splits = (int)std::min<size_t>((size_t)splits, (split_bytes - head) / per_split);
     if (splits < 1) splits = 1;
     a.tiles_per_split = (a.ntiles + splits - 1) / splits;
     splits = (a.ntiles + a.tiles_per_split - 1) / a.tiles_per_split;
-    a.part_key = static_cast<float*>(split_scratch);
-    a.part_idx = reinterpret_cast<int32_t*>(static_cast<char*>(split_scratch) +
+    a.tile_done = static_cast<int*>(split_scratch);
+    a.part_key = reinterpret_cast<float*>(static_cast<char*>(split_scratch) + head);
+    a.part_idx = reinterpret_cast<int32_t*>(static_cast<char*>(split_scratch) + head +
                                             (size_t)splits * nq * kK * 4);
     a.err = d_err;
     const size_t smem = entry_smem_bytes(dim);
     cudaError_t e = cudaFuncSetAttribute(entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
+    if (splits > 1) {
+        e = cudaMemsetAsync(a.tile_done, 0, head, st);
+        if (e != cudaSuccess) return e;
+    }
     entry_kernel<<<dim3((unsigned)((nq + kM - 1) / kM), (unsigned)splits), 128, smem, st>>>(a);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    e = cudaGetLastError();
-    if (e != cudaSuccess || splits == 1) return e;
-    entry_merge<<<(nq + 3) / 4, 128, 0, st>>>(a.part_key, a.part_idx, splits, nq, d_queries, qld,
-                                              dim, d_ids, d_out_ids, d_out_d);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return cudaGetLastError();
 }

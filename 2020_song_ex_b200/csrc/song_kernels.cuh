@@ -93,7 +93,9 @@ cudaError_t build_entry_tables(const float* d_base, int ld, int dim, const int32
 // wait gives up.
 // split_scratch (nullable, split_bytes long; entry_split_scratch_bytes(nq,
 // num_sms) is enough for the widest split) lets the hub tiles of each 128
-// queries spread over several CTAs, whose lists are merged afterwards.
+// queries spread over several CTAs; the last CTA of each 128 queries merges
+// their lists (the scratch also holds the arrival counters, zeroed by an
+// asynchronous memset on the stream before each launch).
 constexpr int kEntrySplits = 16;
 size_t entry_split_scratch_bytes(int nq, int num_sms);
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
