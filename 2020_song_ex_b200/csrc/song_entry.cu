@@ -298,27 +298,48 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
         if (is_last) {
             __threadfence();
             if (q < a.nq) {
-                int pos[kEntrySplits];
+                // list heads in registers (every split's first entry loaded at once);
+                // each step reloads only the winner's next entry
                 const int S = (int)gridDim.y;
-                for (int sp = 0; sp < S; ++sp) pos[sp] = 0;
+                float hk[kEntrySplits];
+                int hx[kEntrySplits], pos[kEntrySplits];
+#pragma unroll
+                for (int sp = 0; sp < kEntrySplits; ++sp) {
+                    pos[sp] = 0;
+                    hx[sp] = -1;
+                    hk[sp] = INFINITY;
+                    if (sp < S) {
+                        const size_t o = ((size_t)sp * a.nq + q) * kK;
+                        hx[sp] = __ldcg(a.part_idx + o);
+                        hk[sp] = __ldcg(a.part_key + o);
+                    }
+                }
                 for (int i = 0; i < kK; ++i) {
                     float bk = INFINITY;
                     int bi = INT_MAX, bs = -1;
-                    for (int sp = 0; sp < S; ++sp) {
-                        if (pos[sp] >= kK) continue;
-                        const size_t o = ((size_t)sp * a.nq + q) * kK + pos[sp];
-                        const int idx = __ldcg(a.part_idx + o);
-                        if (idx < 0) continue;
-                        const float key = __ldcg(a.part_key + o);
-                        if (key < bk || (key == bk && idx < bi)) {
-                            bk = key;
-                            bi = idx;
+#pragma unroll
+                    for (int sp = 0; sp < kEntrySplits; ++sp) {
+                        if (hx[sp] >= 0 && (hk[sp] < bk || (hk[sp] == bk && hx[sp] < bi))) {
+                            bk = hk[sp];
+                            bi = hx[sp];
                             bs = sp;
                         }
                     }
-                    if (bs >= 0) ++pos[bs];
                     a.out_ids[(size_t)q * kK + i] = bs >= 0 ? __ldg(a.hub_ids + bi) : -1;
                     a.out_d[(size_t)q * kK + i] = bs >= 0 ? fmaxf(qn + bk, 0.0f) : INFINITY;
+#pragma unroll
+                    for (int sp = 0; sp < kEntrySplits; ++sp) {
+                        if (sp == bs) {
+                            ++pos[sp];
+                            hx[sp] = -1;
+                            hk[sp] = INFINITY;
+                            if (pos[sp] < kK) {
+                                const size_t o = ((size_t)sp * a.nq + q) * kK + pos[sp];
+                                hx[sp] = __ldcg(a.part_idx + o);
+                                hk[sp] = __ldcg(a.part_key + o);
+                            }
+                        }
+                    }
                 }
             }
         }
