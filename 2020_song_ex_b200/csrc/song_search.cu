@@ -1410,22 +1410,22 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 #include "song_serve_kernel.inc"
 
 // Launch shape of a search_kernel instance.  Queues of up to 1024 slots run
-// in CTAs of 4 warps with at most 80 registers per thread, so that 6 CTAs
-// (24 warps) fit an SM -- the search is latency-bound and gains from every
-// resident query.  The plain and precision searches (LM = 0, queues of
-// hundreds of slots) keep their ids in TMEM (TM), one warp per TMEM lane
-// quarter: ids in shared memory would cost a third of the resident warps at
-// ef 512.  Learned searches run short queues, whose ids fit shared memory
-// without costing warps, and there an id access is one shared-memory load
-// instead of a TMEM round trip (measured 11 % faster).  The learned-model
-// and 256-float-query instances hold more live state; they get 96 registers
-// (5 CTAs, 20 warps) instead of spilling.  Larger queues keep the ids in
-// shared memory, up to 8 warps per CTA.
+// in CTAs of 4 warps with at most 96 registers per thread, so that 5 CTAs
+// (20 warps) fit an SM.  The search is latency-bound and gains from every
+// resident query, but not at the price of spills: capped at 80 registers (6
+// CTAs) the plain and entry-only instances spilled 100-190 bytes and ran
+// 16 % (plain) and 13 % (learned) slower.  The plain and precision searches
+// (LM = 0, queues of hundreds of slots) keep their ids in TMEM (TM), one warp
+// per TMEM lane quarter: ids in shared memory would cost a third of the
+// resident warps at ef 512.  Learned searches run short queues, whose ids fit
+// shared memory without costing warps, and there an id access is one
+// shared-memory load instead of a TMEM round trip (measured 11 % faster).
+// Larger queues keep the ids in shared memory, up to 8 warps per CTA.
 template <int KIND, int NE, int GPL, int DT, int LM>
 struct KernelShape {
     static constexpr int kTM = (GPL == 1 && LM == 0) ? 1 : 0;
     static constexpr int kThreads = GPL == 1 ? 128 : 256;
-    static constexpr int kMinBlocks = GPL == 1 ? ((LM == 1 || LM == 2 || NE >= 8) ? 5 : 6) : 1;
+    static constexpr int kMinBlocks = GPL == 1 ? 5 : 1;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
 };
 
