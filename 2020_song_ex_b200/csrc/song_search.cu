@@ -1420,12 +1420,15 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 // resident warps at ef 512.  Learned searches run short queues, whose ids fit
 // shared memory without costing warps, and there an id access is one
 // shared-memory load instead of a TMEM round trip (measured 11 % faster).
-// Larger queues keep the ids in shared memory, up to 8 warps per CTA.
+// The trace and learned-stop instances (LM = 1, 2: checkpoint features, a
+// running top-k) still spilled at 96 registers; they get 128 (4 CTAs, 16
+// warps), measured 13-16 % faster.  Larger queues keep the ids in shared
+// memory, up to 8 warps per CTA.
 template <int KIND, int NE, int GPL, int DT, int LM>
 struct KernelShape {
     static constexpr int kTM = (GPL == 1 && LM == 0) ? 1 : 0;
     static constexpr int kThreads = GPL == 1 ? 128 : 256;
-    static constexpr int kMinBlocks = GPL == 1 ? 5 : 1;
+    static constexpr int kMinBlocks = GPL == 1 ? ((LM == 1 || LM == 2) ? 4 : 5) : 1;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
 };
 
