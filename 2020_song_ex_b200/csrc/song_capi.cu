@@ -72,16 +72,11 @@ struct song_index {
     int32_t* d_entry_ids = nullptr;
     __nv_bfloat16* d_entry_tiles = nullptr;
     float* d_entry_norm = nullptr;
-    // exact visited bitmaps of the Graph::search mode, one per resident warp
-    uint32_t* d_visited = nullptr;
-    size_t visited_cap = 0;
-    // per-query entry candidates of a launch (grown on demand)
-    int32_t* d_ecand = nullptr;
-    size_t ecand_cap = 0;
-    float* d_edist = nullptr;
-    size_t edist_cap = 0;
-    void* d_esplit = nullptr;  // split scratch of the entry stage (grown on demand)
-    size_t esplit_cap = 0;
+    // Per-call device scratch (the entry stage's candidates and split lists,
+    // the Graph::search visited bitmaps) comes from this stream-ordered pool:
+    // allocated on the call's stream and freed on it after the launches that
+    // use it, so searches of one index on different streams share no buffer.
+    cudaMemPool_t pool = nullptr;
     // learned entry / stop models
     bool has_model = false;
     bool model_staged = false;  // the entry model scores the entry stage's candidates
@@ -165,10 +160,7 @@ void free_index(song_index* x) {
     cudaFree(x->d_entry_ids);
     cudaFree(x->d_entry_tiles);
     cudaFree(x->d_entry_norm);
-    cudaFree(x->d_ecand);
-    cudaFree(x->d_visited);
-    cudaFree(x->d_esplit);
-    cudaFree(x->d_edist);
+    if (x->pool) cudaMemPoolDestroy(x->pool);  // released once its async frees complete
     cudaFree(x->d_bf16);
     cudaFree(x->d_fp8);
     cudaFree(x->d_fp8_scale);
@@ -212,6 +204,17 @@ song_status create_common(int kind, const void* rows, int64_t n, int dim, const 
     if (e == cudaSuccess) e = cudaMalloc(&x->d_counter, kCounterRing * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&x->d_err, 256);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        cudaMemPoolProps pp = {};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = x->device;
+        e = cudaMemPoolCreate(&x->pool, &pp);
+    }
+    if (e == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;  // keep freed blocks for the next call
+        e = cudaMemPoolSetAttribute(x->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (e == cudaSuccess) e = cudaEventCreate(&x->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&x->ev1);
     if (e == cudaSuccess && x->ld != dim) e = cudaMemset(x->d_base, 0, (size_t)n * row_bytes);
@@ -250,6 +253,32 @@ cudaError_t grow(T** ptr, size_t* cap, size_t bytes) {
     if (e == cudaSuccess) *cap = bytes;
     return e;
 }
+
+// Device scratch of one call, from the index's pool on the call's stream;
+// every block is freed on that stream when the object goes out of scope,
+// i.e. after the launches the call made.
+struct CallScratch {
+    song_index* x;
+    cudaStream_t st;
+    void* p[4] = {nullptr, nullptr, nullptr, nullptr};
+    int n = 0;
+    CallScratch(song_index* idx, cudaStream_t s) : x(idx), st(s) {}
+    CallScratch(const CallScratch&) = delete;
+    CallScratch& operator=(const CallScratch&) = delete;
+    template <typename T>
+    cudaError_t get(T** out, size_t bytes) {
+        if (n == 4) return cudaErrorInvalidValue;
+        void* q = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&q, bytes, x->pool, st);
+        if (e != cudaSuccess) return e;
+        p[n++] = q;
+        *out = static_cast<T*>(q);
+        return cudaSuccess;
+    }
+    ~CallScratch() {
+        for (int i = 0; i < n; ++i) cudaFreeAsync(p[i], st);
+    }
+};
 
 // Build the entry stage's tables for hub node ids `hubs` (device, stream-ordered).
 song_status attach_entry_hubs(song_index* x, const std::vector<int32_t>& hubs) {
@@ -290,11 +319,13 @@ song_status attach_entry_hubs(song_index* x, const std::vector<int32_t>& hubs) {
 // The entry stage for nq queries at d_q: ids/dists [nq x kEntryK].
 song_status run_entry(song_index* x, const void* d_q, int nq, int32_t* d_ids, float* d_d,
                       cudaStream_t st) {
-    SONG_CUDA(grow(&x->d_esplit, &x->esplit_cap, song::entry_split_scratch_bytes(nq, x->num_sms)),
-              "entry split scratch");
+    CallScratch cs(x, st);
+    const size_t split_bytes = song::entry_split_scratch_bytes(nq, x->num_sms);
+    void* split = nullptr;
+    SONG_CUDA(cs.get(&split, split_bytes), "entry split scratch");
     cudaError_t e = song::launch_entry((const float*)d_q, x->dim, nq, x->dim, x->d_entry_tiles,
                                        x->d_entry_norm, x->d_entry_ids, x->entry_hpad, d_ids, d_d,
-                                       x->d_err, st, x->d_esplit, x->esplit_cap, x->num_sms);
+                                       x->d_err, st, split, split_bytes, x->num_sms);
     if (e != cudaSuccess) return cuda_fail(e, "entry launch");
     return SONG_OK;
 }
@@ -392,14 +423,17 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
 }
 
 song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
+    CallScratch cs(x, st);
     if (a.lm == 2 && x->model_staged && a.qseeds == nullptr && a.ecand == nullptr && a.nq > 0) {
         // learned search: the entry stage first, on the same stream
         const size_t cells = (size_t)a.nq * song::kEntryK;
-        SONG_CUDA(grow(&x->d_ecand, &x->ecand_cap, cells * 4), "entry candidates alloc");
-        SONG_CUDA(grow(&x->d_edist, &x->edist_cap, cells * 4), "entry distances alloc");
-        if (song_status s = run_entry(x, a.queries, a.nq, x->d_ecand, x->d_edist, st)) return s;
-        a.ecand = x->d_ecand;
-        a.edist = x->d_edist;
+        int32_t* ecand = nullptr;
+        float* edist = nullptr;
+        SONG_CUDA(cs.get(&ecand, cells * 4), "entry candidates alloc");
+        SONG_CUDA(cs.get(&edist, cells * 4), "entry distances alloc");
+        if (song_status s = run_entry(x, a.queries, a.nq, ecand, edist, st)) return s;
+        a.ecand = ecand;
+        a.edist = edist;
     }
     unsigned* ctr = x->d_counter + (x->counter_next++ % kCounterRing);
     a.counter = ctr;
@@ -749,13 +783,15 @@ song_status graph_search_launch(song_index* x, const float* d_q, int nq, int k, 
     const int64_t warps = song::graph_search_resident_warps(x->dim, ef, x->num_sms, x->device);
     if (warps < 4) return fail(SONG_ERR_UNSUPPORTED, "Graph::search mode: per-query state does not fit");
     const int64_t vwords = (x->n + 31) / 32;
-    SONG_CUDA(grow(&x->d_visited, &x->visited_cap, (size_t)warps * vwords * 4), "visited bitmaps");
+    CallScratch cs(x, st);
+    uint32_t* visited = nullptr;
+    SONG_CUDA(cs.get(&visited, (size_t)warps * vwords * 4), "visited bitmaps");
     unsigned* ctr = x->d_counter + (x->counter_next++ % kCounterRing);
     SONG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), st), "counter reset");
     cudaError_t e = song::launch_graph_search((const float*)x->d_base, x->ld, x->dim, x->d_adj,
                                               x->p.block_size, x->n, d_q, nq, k, ef,
                                               x->p.n_multiprobe, d_ids, d_tr, ctr, x->d_err,
-                                              x->d_visited, warps, x->num_sms, st);
+                                              visited, warps, x->num_sms, st);
     if (e != cudaSuccess) return cuda_fail(e, "Graph::search launch");
     return SONG_OK;
 }

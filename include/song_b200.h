@@ -187,10 +187,12 @@ song_status song_graph_search_device(song_index* index, const float* d_queries, 
  * Device-resident search: d_queries (FP32 or u32 codes, by index kind),
  * d_ids[nq x k] and d_traces (nullable) are device pointers; the call is
  * asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).
- * Same clamp and results as song_gpu_search.  The searches of one index
- * share its device work buffers (the query counter, the entry stage's
- * candidates and split lists): issue them on one stream, or give each
- * stream its own index, so that they do not overlap on the GPU.
+ * Same clamp and results as song_gpu_search.  Searches of one index may
+ * run on different streams at the same time: each launch takes its own work
+ * counter (a ring of 1024 per index) and its own scratch (entry-stage lists,
+ * Graph::search bitmaps) from the index's stream-ordered memory pool, freed
+ * on the launching stream.  Host calls on one index are serialised by a
+ * lock.
  */
 song_status song_search_device(song_index* index, const void* d_queries, int nq, int k,
                                int ef_search, int32_t* d_ids, song_query_trace* d_traces,

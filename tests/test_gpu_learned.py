@@ -152,3 +152,30 @@ def test_bloom_hashes_option(cuda, song, ds):
     with pytest.raises(song.SongError):
         song.gpu_search_ex(g, song.SearchOpts(bloom_hashes=2), m.queries, nq, 10, 64)
     g.close()
+
+
+def test_concurrent_streams_share_no_buffers(cuda, song, ds):
+    """Searches of one index issued on two streams at once -- learned ones,
+    each with its own entry-stage launch, and plain ones -- return exactly
+    what the same queries return one call at a time: every launch takes its
+    own work counter and its own entry-stage scratch."""
+    torch = importlib.import_module("torch")
+    m, g, gt, rep = _setup(song, ds, n=30000, nq=400, ntrain=2000)
+    nq = m.queries.shape[0]
+    h = nq // 2
+    dq = torch.from_numpy(m.queries).cuda()
+    for opts, ef in ((song.SearchOpts(learned=True, stop_threshold=1.0, beam=2), 64),
+                     (song.SearchOpts(), 128)):
+        ref = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+        song.search_device_ex(g, opts, dq, nq, 10, ef, ref, None, None)
+        torch.cuda.synchronize()
+        s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+        for _ in range(3):
+            o1 = torch.full((h, 10), -7, dtype=torch.int32, device="cuda")
+            o2 = torch.full((nq - h, 10), -7, dtype=torch.int32, device="cuda")
+            torch.cuda.synchronize()
+            song.search_device_ex(g, opts, dq[:h], h, 10, ef, o1, None, None, stream=s1)
+            song.search_device_ex(g, opts, dq[h:], nq - h, 10, ef, o2, None, None, stream=s2)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(torch.cat([o1, o2]).cpu().numpy(), ref.cpu().numpy())
+    g.close()
