@@ -627,15 +627,15 @@ __device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int
 // Otherwise the extraction is undone and the trims and drains are replayed.
 // `scratch` (TM = 1: at least cap ints of shared memory) holds the slots of
 // the extracted results; with TM = 0 the free candidate id array does.
-template <int GPL, int TM>
-__device__ __forceinline__ int finish(Queue<GPL, TM>& res, Queue<GPL, TM>& cand, int k,
+template <int GPL, int TM, int TMC>
+__device__ __forceinline__ int finish(Queue<GPL, TM>& res, Queue<GPL, TMC>& cand, int k,
                                       int32_t* out, float* outd, int lane, int* scratch) {
     const int ng = (res.sz + 31) >> 5;
     for (int g = 0; g < ng; ++g) group_update<true>(res, g, lane);
     const int cnt = res.sz < k ? res.sz : k;
     const int take = res.sz < k + 1 ? res.sz : k + 1;
     unsigned* xv = reinterpret_cast<unsigned*>(cand.d);  // extracted distance bits
-    int* xs = TM ? scratch : cand.id;                    // their slots
+    int* xs = TMC ? scratch : cand.id;                   // their slots
     for (int i = 0; i < take; ++i) {
         unsigned mb, mi;
         root_min(res, mb, mi);
@@ -780,9 +780,9 @@ __device__ __forceinline__ float l2_lowp(const SearchArgs& a, const float* sq, i
 // Precision form, final step: exact FP32 distances of every entry of the
 // results queue (FP32 rows, 8 lanes per row), then the k smallest by
 // (distance, id) in ascending order, -1 padded.
-template <int GPL, int TM>
+template <int GPL, int TM, int TMC>
 __device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL, TM>& res,
-                                             Queue<GPL, TM>& cand, const float* sq, int32_t* out,
+                                             Queue<GPL, TMC>& cand, const float* sq, int32_t* out,
                                              float* outd, int lane) {
     const int m = res.sz;
     float* rd = cand.d;
@@ -1008,18 +1008,20 @@ __device__ __forceinline__ unsigned fkey(float x) {
 // BF16 / FP8 rows (KIND 0, query in shared memory, FP32 re-rank at the end).
 // LM: 0 plain; 1 learning traces; 2 learned entry and stop; 3 learned entry
 // only (the instance for a stop model that cannot fire).
-// TM = 1: the queue ids live in this warp's TMEM lanes from column `tbase`
-// (candidates in columns tbase .. tbase+G-1, results in the next G, with G =
-// ceil(cap / 32)); the per-warp shared-memory layout then has no id arrays.
-template <int KIND, int NE, int GPL, int DT, int LM, int TM = 0>
+// TM = 1: the result ids live in this warp's TMEM lanes from column `tbase`
+// (G = ceil(cap / 32) columns); TMC = 1: so do the candidate ids, in the G
+// columns before them.  The per-warp shared-memory layout then has no id
+// array for that queue.
+template <int KIND, int NE, int GPL, int DT, int LM, int TM = 0, int TMC = TM>
 __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsigned char* ws,
                                              int lane, uint32_t tbase = 0) {
-    Queue<GPL, TM> cand, res;
+    Queue<GPL, TMC> cand;
+    Queue<GPL, TM> res;
     const uint32_t ngrp = (uint32_t)((a.cap + 31) >> 5);
     q_init(cand, reinterpret_cast<float*>(ws + a.cd_off), reinterpret_cast<int*>(ws + a.ci_off),
            tbase, a.cap);
     q_init(res, reinterpret_cast<float*>(ws + a.rd_off), reinterpret_cast<int*>(ws + a.ri_off),
-           tbase + ngrp, a.cap);
+           tbase + (TMC ? ngrp : 0u), a.cap);
     uint64_t* bloom = reinterpret_cast<uint64_t*>(ws + a.bl_off);
     float* sq = reinterpret_cast<float*>(ws + a.q_off);
     int* rows = reinterpret_cast<int*>(ws + a.rows_off);
@@ -1415,9 +1417,12 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 // resident query, but not at the price of spills: capped at 80 registers (6
 // CTAs) the plain and entry-only instances spilled 100-190 bytes and ran
 // 16 % (plain) and 13 % (learned) slower.  The plain and precision searches
-// (LM = 0, queues of hundreds of slots) keep their ids in TMEM (TM), one warp
-// per TMEM lane quarter: ids in shared memory would cost a third of the
-// resident warps at ef 512.  Learned searches run short queues, whose ids fit
+// (LM = 0, queues of hundreds of slots) keep their result ids in TMEM (TM),
+// one warp per TMEM lane quarter, and their candidate ids (the hotter queue:
+// every expansion pops it) in shared memory: at ef 512 with a 512-word Bloom
+// filter that still fits 5 CTAs per SM, where both id arrays in shared
+// memory would not (measured 4-5 % faster than both in TMEM, 11 % faster
+// than both in shared memory).  Learned searches run short queues, whose ids fit
 // shared memory without costing warps, and there an id access is one
 // shared-memory load instead of a TMEM round trip (measured 11 % faster).
 // The trace and learned-stop instances (LM = 1, 2: checkpoint features, a
@@ -1426,7 +1431,8 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 // memory, up to 8 warps per CTA.
 template <int KIND, int NE, int GPL, int DT, int LM>
 struct KernelShape {
-    static constexpr int kTM = (GPL == 1 && LM == 0) ? 1 : 0;
+    static constexpr int kTM = (GPL == 1 && LM == 0) ? 1 : 0;   // result ids in TMEM
+    static constexpr int kTMC = 0;                              // candidate ids in TMEM
     static constexpr int kThreads = GPL == 1 ? 128 : 256;
     static constexpr int kMinBlocks = GPL == 1 ? ((LM == 1 || LM == 2) ? 4 : 5) : 1;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
@@ -1438,6 +1444,7 @@ __global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads)
     search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int TM = KernelShape<KIND, NE, GPL, DT, LM>::kTM;
+    constexpr int TMC = KernelShape<KIND, NE, GPL, DT, LM>::kTMC;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ws = smem + (size_t)warp * a.warp_smem;
     uint32_t tbase = 0;
@@ -1460,7 +1467,7 @@ __global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads)
         if (lane == 0) qid = (int)atomicAdd(a.counter, 1u);
         qid = __shfl_sync(FULL, qid, 0);
         if (qid >= a.nq) break;
-        search_query<KIND, NE, GPL, DT, LM, TM>(a, qid, ws, lane, tbase);
+        search_query<KIND, NE, GPL, DT, LM, TM, TMC>(a, qid, ws, lane, tbase);
     }
     if constexpr (TM) {  // every warp is done with TMEM before it is freed
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1477,7 +1484,8 @@ using KernelFn = void (*)(const SearchArgs);
 // A chosen kernel instance and its launch shape.
 struct KernelSel {
     KernelFn fn = nullptr;
-    int tm = 0;
+    int tm = 0;   // result ids in TMEM (the CTA allocates tensor memory)
+    int tmc = 0;  // candidate ids in TMEM too
     int threads = 256;
     bool query_smem = true;
 };
@@ -1488,6 +1496,7 @@ KernelSel ksel() {
     KernelSel k;
     k.fn = search_kernel<KIND, NE, GPL, DT, LM>;
     k.tm = S::kTM;
+    k.tmc = S::kTMC;
     k.threads = S::kThreads;
     k.query_smem = S::kQuerySmem;
     return k;
@@ -1609,20 +1618,21 @@ cudaError_t tm_ctas_per_sm(KernelFn fn, int dev, int warps, size_t dyn_smem, int
 }
 
 // Per-warp shared memory of the TMEM-id kernels: [query if kept in shared
-// memory][32-entry row list][candidate distances][result distances][Bloom
-// filter], the Bloom region being at least cap ints because finish() keeps
-// the extracted slots there once the search is over.
-void tm_layout(int query_floats, SearchArgs* a) {
+// memory][32-entry row list][candidate distances][candidate ids, unless they
+// are in TMEM too][result distances][Bloom filter], the Bloom region being at
+// least cap ints because finish() may keep the extracted slots there once
+// the search is over.
+void tm_layout(int query_floats, bool cand_in_tmem, SearchArgs* a) {
     const int capr = round_up(a->cap, 32);
     a->q_off = 0;
     a->rows_off = round_up(query_floats * 4, 16);
     a->cd_off = a->rows_off + 128;
-    a->rd_off = a->cd_off + capr * 4;
-    a->ci_off = 0;
+    a->ci_off = cand_in_tmem ? 0 : a->cd_off + capr * 4;
+    a->rd_off = cand_in_tmem ? a->cd_off + capr * 4 : a->ci_off + capr * 4;
     a->ri_off = 0;
     a->bl_off = round_up(a->rd_off + capr * 4, 16);
     a->warp_smem = round_up(a->bl_off + std::max(a->bf_words * 8, capr * 4), 16);
-    a->tm_warp_cols = 2 * (capr / 32);
+    a->tm_warp_cols = (cand_in_tmem ? 2 : 1) * (capr / 32);
 }
 
 }  // namespace
@@ -1739,7 +1749,7 @@ cudaError_t launch_search(int kind, const SearchArgs& args, int num_sms, cudaStr
     if (ks.tm) {
         // ids in TMEM: CTAs of 4 warps, one per lane quarter; 2 * ceil(cap/32)
         // columns per warp, allocated per CTA in a power of two >= 32
-        tm_layout(ks.query_smem ? a.qdim : 0, &a);
+        tm_layout(ks.query_smem ? a.qdim : 0, ks.tmc != 0, &a);
         warps = ks.threads / 32;
         int cols = 32;
         while (cols < a.tm_warp_cols * (warps / 4)) cols <<= 1;
