@@ -1422,7 +1422,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 // every expansion pops it) in shared memory: at ef 512 with a 512-word Bloom
 // filter that still fits 5 CTAs per SM, where both id arrays in shared
 // memory would not (measured 4-5 % faster than both in TMEM, 11 % faster
-// than both in shared memory).  Learned searches run short queues, whose ids fit
+// than both in shared memory).  Both placements are compiled; the launcher
+// takes the candidate ids into TMEM too when shared memory would otherwise
+// cost resident CTAs (large queues and Bloom filters).  Learned searches run short queues, whose ids fit
 // shared memory without costing warps, and there an id access is one
 // shared-memory load instead of a TMEM round trip (measured 11 % faster).
 // The trace and learned-stop instances (LM = 1, 2: checkpoint features, a
@@ -1432,19 +1434,19 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
 template <int KIND, int NE, int GPL, int DT, int LM>
 struct KernelShape {
     static constexpr int kTM = (GPL == 1 && LM == 0) ? 1 : 0;   // result ids in TMEM
-    static constexpr int kTMC = 0;                              // candidate ids in TMEM
     static constexpr int kThreads = GPL == 1 ? 128 : 256;
     static constexpr int kMinBlocks = GPL == 1 ? ((LM == 1 || LM == 2) ? 4 : 5) : 1;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
 };
 
-template <int KIND, int NE, int GPL, int DT, int LM = 0>
+// TMC = 1 (TM instances only): the candidate ids in TMEM as well.
+template <int KIND, int NE, int GPL, int DT, int LM = 0, int TMC = 0>
 __global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads),
                                   (KernelShape<KIND, NE, GPL, DT, LM>::kMinBlocks))
     search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int TM = KernelShape<KIND, NE, GPL, DT, LM>::kTM;
-    constexpr int TMC = KernelShape<KIND, NE, GPL, DT, LM>::kTMC;
+    static_assert(TM || !TMC, "candidate ids in TMEM need a TMEM allocation");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ws = smem + (size_t)warp * a.warp_smem;
     uint32_t tbase = 0;
@@ -1483,9 +1485,9 @@ using KernelFn = void (*)(const SearchArgs);
 
 // A chosen kernel instance and its launch shape.
 struct KernelSel {
-    KernelFn fn = nullptr;
-    int tm = 0;   // result ids in TMEM (the CTA allocates tensor memory)
-    int tmc = 0;  // candidate ids in TMEM too
+    KernelFn fn = nullptr;      // candidate ids in shared memory
+    KernelFn fn_tmc = nullptr;  // tm only: the candidate ids in TMEM too
+    int tm = 0;                 // result ids in TMEM (the CTA allocates tensor memory)
     int threads = 256;
     bool query_smem = true;
 };
@@ -1494,9 +1496,9 @@ template <int KIND, int NE, int GPL, int DT, int LM = 0>
 KernelSel ksel() {
     using S = KernelShape<KIND, NE, GPL, DT, LM>;
     KernelSel k;
-    k.fn = search_kernel<KIND, NE, GPL, DT, LM>;
+    k.fn = search_kernel<KIND, NE, GPL, DT, LM, 0>;
+    if constexpr (S::kTM) k.fn_tmc = search_kernel<KIND, NE, GPL, DT, LM, 1>;
     k.tm = S::kTM;
-    k.tmc = S::kTMC;
     k.threads = S::kThreads;
     k.query_smem = S::kQuerySmem;
     return k;
@@ -1746,15 +1748,37 @@ cudaError_t launch_search(int kind, const SearchArgs& args, int num_sms, cudaStr
     e = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
     int warps;
+    int tm_per_sm = 0;
     if (ks.tm) {
-        // ids in TMEM: CTAs of 4 warps, one per lane quarter; 2 * ceil(cap/32)
-        // columns per warp, allocated per CTA in a power of two >= 32
-        tm_layout(ks.query_smem ? a.qdim : 0, ks.tmc != 0, &a);
+        // ids in TMEM: CTAs of 4 warps, one per lane quarter; ceil(cap/32)
+        // columns per warp and queue, allocated per CTA in a power of two >= 32.
+        // The candidate ids go to shared memory unless that costs resident CTAs
+        // (large queues and Bloom filters), then to TMEM as well.
         warps = ks.threads / 32;
-        int cols = 32;
-        while (cols < a.tm_warp_cols * (warps / 4)) cols <<= 1;
-        if (cols > 512) return cudaErrorInvalidConfiguration;
-        a.tm_cols = cols;
+        auto shape = [&](bool cand_tm, SearchArgs* s2, int* per_sm) -> cudaError_t {
+            tm_layout(ks.query_smem ? s2->qdim : 0, cand_tm, s2);
+            int cols = 32;
+            while (cols < s2->tm_warp_cols * (warps / 4)) cols <<= 1;
+            s2->tm_cols = cols;
+            *per_sm = 0;
+            if (cols > 512 || (size_t)warps * s2->warp_smem > (size_t)smem_optin) return cudaSuccess;
+            return tm_ctas_per_sm(cand_tm ? ks.fn_tmc : ks.fn, dev, warps, (size_t)warps * s2->warp_smem,
+                                  cols, per_sm);
+        };
+        SearchArgs a0 = a, a1 = a;
+        int p0 = 0, p1 = 0;
+        e = shape(false, &a0, &p0);
+        if (e == cudaSuccess) e = shape(true, &a1, &p1);
+        if (e != cudaSuccess) return e;
+        if (p1 > p0) {
+            a = a1;
+            fn = ks.fn_tmc;
+            tm_per_sm = p1;
+        } else {
+            a = a0;
+            tm_per_sm = p0;
+        }
+        if (tm_per_sm < 1) return cudaErrorInvalidConfiguration;
     } else {
         // Up to 8 warps per CTA while the CTA's shared memory stays within a
         // quarter of the opt-in limit, so several CTAs can share an SM.
@@ -1767,7 +1791,7 @@ cudaError_t launch_search(int kind, const SearchArgs& args, int num_sms, cudaStr
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     if (ks.tm) {
-        e = tm_ctas_per_sm(fn, dev, warps, smem, a.tm_cols, &per_sm);
+        per_sm = tm_per_sm;
     } else {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, warps * 32, smem);
     }
