@@ -598,7 +598,7 @@ class LearnParams:
     batch: int = 4096
     lr: float = 2e-3
     seed: int = 2020
-    entry_hubs: int = 4096  # hub set of the tensor-core entry stage; 0 = 24 in-kernel hubs
+    entry_hubs: int = 8192  # hub set of the tensor-core entry stage; 0 = 24 in-kernel hubs
 
     def _c(self) -> _LearnParams:
         return _LearnParams(self.k, self.ef, self.ckpt_every, self.min_expansions, self.max_ckpt,

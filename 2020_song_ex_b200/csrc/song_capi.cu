@@ -879,7 +879,7 @@ void song_learn_params_default(song_learn_params* p) {
     p->stop_steps = 3000;
     p->batch = 4096;
     p->lr = 2e-3f;
-    p->entry_hubs = 4096;
+    p->entry_hubs = 8192;
     p->seed = 2020;
 }
 

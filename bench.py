@@ -406,9 +406,9 @@ def run_ours(args, ws, rank, local):
             ids_l = d_ids.cpu().numpy()
             song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
             stream.synchronize()
-            # gathered rows + the entry stage's hub tiles (4096 x 128 BF16 per 128 queries)
+            # gathered rows + the entry stage's hub tiles (hubs x dim BF16 per 128 queries)
             l_bytes = float(bytes_per_query(d_tr.cpu().numpy(), K, row_bytes).sum()) + \
-                (NQ + 127) // 128 * 4096 * DIM * 2
+                (NQ + 127) // 128 * int(rep.get("n_hubs", 0) or 0) * DIM * 2
             copts = lopts._c()
 
             def host_learned():
@@ -420,7 +420,7 @@ def run_ours(args, ws, rank, local):
 
             l_e2e_s = timed_host(torch, dist, ws, dev, args.steps, args.warmup, host_learned)
             learned = {
-                "form": "tensor-core entry stage (4096 hubs) + learned entry/stop model, byte rows",
+                "form": f"tensor-core entry stage ({int(rep.get('n_hubs', 0) or 0)} hubs) + learned entry/stop model, byte rows",
                 "precision": "u8 rows (exact for these integer vectors)" if row_bytes < DIM * 4 else "fp32",
                 "threshold": lbest["threshold"], "beam": lbest["beam"],
                 "bloom_hashes": lbest["bloom_hashes"], "ef": lef,

@@ -333,7 +333,7 @@ typedef struct song_learn_params {
     int batch;           /* minibatch (default 4096)                                       */
     float lr;            /* Adam learning rate (default 2e-3)                              */
     unsigned seed;
-    int entry_hubs;      /* hub set of the tensor-core entry stage (default 4096; dim <= 288).
+    int entry_hubs;      /* hub set of the tensor-core entry stage (default 8192; dim <= 288).
                             0: the entry model scores 24 farthest-point hubs instead   */
 } song_learn_params;
 
