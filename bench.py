@@ -453,7 +453,7 @@ def run_ours(args, ws, rank, local):
         achieved = launch_bytes / avg_kern_s / 1e9
         traffic, traffic_src = ncu_traffic(ef, best["bf_words"])
         roof_plain = {
-            "kernel": "plain search_kernel<0,4,1,0,0> (bit-exact form)",
+            "kernel": "plain search_kernel<0,4,1,0,0,0> (bit-exact form)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
             "traffic": traffic, "traffic_source": traffic_src,
@@ -469,9 +469,9 @@ def run_ours(args, ws, rank, local):
             la = learned["algorithmic_bytes_per_launch"] / (learned["kernel_ms_avg"] / 1e3) / 1e9
             lt, lsrc = ncu_traffic(learned["ef"], best["bf_words"], form="learned")
             roof_learned = {
-                "kernel": ("entry_kernel + search_kernel<0,4,1,0,3> (entry model; the stop cannot fire)"
+                "kernel": ("entry_kernel + search_kernel<0,4,1,0,3,0> (entry model; the stop cannot fire)"
                            if learned["threshold"] >= 1.0 else
-                           "entry_kernel + search_kernel<0,4,1,0,2> (entry + stop models)"),
+                           "entry_kernel + search_kernel<0,4,1,0,2,0> (entry + stop models)"),
                 "bound": "hbm", "achieved": round(la, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(la / peak, 4), "peak_kind": peak_kind,
                 "traffic": lt, "traffic_source": lsrc,
