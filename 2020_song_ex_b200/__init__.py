@@ -40,6 +40,9 @@ KIND_HAMMING = 1
 PREC_FP32 = 0
 PREC_BF16 = 1
 PREC_FP8 = 2
+ENTRY_MODEL = 0    # learned entry points: the entry model's top hubs
+ENTRY_NEAREST = 1  # the entry stage's nearest hubs, no model
+ENTRY_SEEDS = 2    # the reference's seeds p*n/N_MULTIPROBE, no entry stage
 
 TRACE_FIELDS = (
     "seed_count", "visited_nodes", "expanded_nodes", "neighbor_slots_scanned",
@@ -71,7 +74,7 @@ class _Timing(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("rerank", C.c_int), ("learned", C.c_int),
                 ("stop_threshold", C.c_float), ("beam", C.c_int), ("bloom_hashes", C.c_int),
-                ("reserved", C.c_int * 2)]
+                ("entry", C.c_int), ("reserved", C.c_int)]
 
 
 @dataclass
@@ -84,10 +87,12 @@ class SearchOpts:
     stop_threshold: float = 0.5
     beam: int = 1  # learned search: 2 expands the two best candidates per step
     bloom_hashes: int = 0  # learned search: Bloom hashes per id (0 = the index's bf_nhash)
+    entry: int = 0  # learned search: ENTRY_MODEL, ENTRY_NEAREST (no model) or ENTRY_SEEDS
 
     def _c(self) -> _Opts:
         return _Opts(int(self.precision), int(bool(self.rerank)), int(bool(self.learned)),
-                     float(self.stop_threshold), int(self.beam), int(self.bloom_hashes))
+                     float(self.stop_threshold), int(self.beam), int(self.bloom_hashes),
+                     int(self.entry))
 
 
 class _LearnParams(C.Structure):

@@ -44,15 +44,28 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel (one nvcc per file), then
+    link the shared library."""
     if not force and not stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
+
+    def compile_one(src: str) -> str:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [NVCC, *FLAGS, *inc, "-c", src, "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, sources()))
     tmp = LIB + ".tmp"
-    cmd = [NVCC, *FLAGS, "-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           *sources(), "-o", tmp]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.check_call(cmd)
+    subprocess.check_call([NVCC, *FLAGS, "-shared", *objs, "-o", tmp])
     os.replace(tmp, LIB)
     return LIB
 

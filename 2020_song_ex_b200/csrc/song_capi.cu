@@ -395,6 +395,17 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
         a->n_hubs = x->model_staged ? 0 : (int)x->hubs.size();
         a->entry_w = x->d_entry_w;
         a->stop_w = x->d_stop_w;
+        if (opts->entry < SONG_ENTRY_MODEL || opts->entry > SONG_ENTRY_SEEDS)
+            return fail(SONG_ERR_INVALID_ARG, "entry must be SONG_ENTRY_MODEL, _NEAREST or _SEEDS");
+        if (opts->entry == SONG_ENTRY_NEAREST) {
+            if (!x->model_staged)
+                return fail(SONG_ERR_INVALID_ARG, "SONG_ENTRY_NEAREST needs the entry stage's hub set");
+            a->entry_w = nullptr;  // the kernel then seeds from the nearest hubs
+        } else if (opts->entry == SONG_ENTRY_SEEDS) {
+            a->entry_w = nullptr;
+            a->n_hubs = 0;
+            a->no_entry_stage = 1;
+        }
         a->ckpt_every = x->ckpt_every;
         a->min_expansions = x->min_expansions;
         a->beam = opts->beam < 1 ? 1 : (opts->beam > 4 ? 4 : opts->beam);
@@ -424,7 +435,8 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
 
 song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
     CallScratch cs(x, st);
-    if (a.lm == 2 && x->model_staged && a.qseeds == nullptr && a.ecand == nullptr && a.nq > 0) {
+    if (a.lm == 2 && x->model_staged && !a.no_entry_stage && a.qseeds == nullptr &&
+        a.ecand == nullptr && a.nq > 0) {
         // learned search: the entry stage first, on the same stream
         const size_t cells = (size_t)a.nq * song::kEntryK;
         int32_t* ecand = nullptr;

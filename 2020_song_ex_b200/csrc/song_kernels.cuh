@@ -51,6 +51,7 @@ struct SearchArgs {
     float* out_dist;         // [nq x k] distance of each output id (nullable)
     // learned entry / stop (lm: 0 off, 1 collect traces of the full search, 2 infer)
     int lm;
+    int no_entry_stage;      // learned searches: 1 = skip the entry stage (reference seeds)
     const int32_t* ecand;    // [nq x kEntryK] entry-stage candidates (hub node ids, -1 = none), or nullptr
     const float* edist;      // [nq x kEntryK] their squared distances
     const int32_t* hubs;     // [n_hubs] entry hub node ids (n_hubs <= kFeat)

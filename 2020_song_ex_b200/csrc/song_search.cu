@@ -602,19 +602,29 @@ __device__ __forceinline__ float l2_u8(const uint8_t* __restrict__ base, int ld,
     return out;
 }
 
-// Hamming distance of this lane's own row: popcount(q ^ b) over W4 uint4
-// (warp_hamming, hashKernelGraph.h:215-224; integer, so order-free).
+// Hamming distance of this lane's own row: popcount(q ^ b) over the dim code
+// words (warp_hamming, hashKernelGraph.h:215-224; integer, so order-free).
+// Rows are W4 uint4 wide; words at or past dim are padding and never count,
+// whatever they hold (the query's are zero, a caller's rows may not be).
 template <int W4>
-__device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int ld,
+__device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int ld, int dim,
                                           const uint4 (&q)[W4], int nb, bool mine) {
     int s = 0;
     if (mine) {
         const uint4* row = reinterpret_cast<const uint4*>(base + (size_t)nb * ld);
 #pragma unroll
         for (int e = 0; e < W4; ++e) {
-            const uint4 x = ld_row(row + e);
-            s += __popc(x.x ^ q[e].x) + __popc(x.y ^ q[e].y) + __popc(x.z ^ q[e].z) +
-                 __popc(x.w ^ q[e].w);
+            if (4 * e < dim) {
+                uint4 x = ld_row(row + e);
+                if (4 * e + 4 > dim) {  // the chunk holding the last word: drop the rest
+                    const int r = dim - 4 * e;
+                    if (r < 2) x.y = q[e].y;
+                    if (r < 3) x.z = q[e].z;
+                    x.w = q[e].w;
+                }
+                s += __popc(x.x ^ q[e].x) + __popc(x.y ^ q[e].y) + __popc(x.z ^ q[e].z) +
+                     __popc(x.w ^ q[e].w);
+            }
         }
     }
     return (float)s;
@@ -1140,7 +1150,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
             }
         } else {
-            d = ham_lane<NE>(reinterpret_cast<const uint32_t*>(a.base), a.ld, qcode, nb,
+            d = ham_lane<NE>(reinterpret_cast<const uint32_t*>(a.base), a.ld, a.dim, qcode, nb,
                              (N >> lane) & 1u);
         }
         return d;

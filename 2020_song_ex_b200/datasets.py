@@ -38,11 +38,14 @@ def _pick(rng: np.random.Generator, n: int, n_comp: int) -> np.ndarray:
 
 
 def int_mixture(n: int, nq: int, dim: int = 128, n_comp: int = 64, sigma: float = 20.0,
-                seed: int = 0, chunk: int = 1 << 18, query_seed=None) -> Mixture:
+                seed: int = 0, chunk: int = 1 << 18, query_seed=None,
+                with_base: bool = True) -> Mixture:
     """Integer-valued FP32 points: centre ~ U[0,255]^dim + N(0, sigma^2), clip, round.
 
     ``query_seed`` draws the queries from the same mixture with a separate
-    generator (independent query sets over one base, e.g. one per GPU).
+    generator (independent query sets over one base, e.g. one per GPU); with
+    it, ``with_base=False`` skips drawing the base (``base`` is then empty)
+    and the queries are the same as with it.
     """
     rng = np.random.default_rng(seed)
     centres = rng.uniform(0.0, 255.0, size=(n_comp, dim))
@@ -57,7 +60,10 @@ def int_mixture(n: int, nq: int, dim: int = 128, n_comp: int = 64, sigma: float 
             out[s:e] = x
         return out
 
-    base = draw(n)
+    if query_seed is not None and not with_base:
+        base = np.zeros((0, dim), dtype=np.float32)
+    else:
+        base = draw(n)
     if query_seed is not None:
         rng = np.random.default_rng(query_seed)
     queries = draw(nq)

@@ -1,28 +1,42 @@
-"""Benchmark: QPS at recall@10 >= 0.95 of the SONG graph search on B200.
+"""Benchmark: QPS at recall@10 >= 0.95 of the SONG graph search on one B200.
 
 Workload (one "step" = one pass of the search over the whole query batch):
 1,000,000 x 128 integer-valued FP32 base vectors from a 1,024-component
 Gaussian mixture (centres U[0,255], sigma 20, clipped and rounded), 10,000
-queries from the same mixture, NSW graph with BLOCK_SIZE 32 (degree 31) built
-on the GPU, k = 10.  Synthetic, seeded stand-in for SIFT1M-shaped data (the
-public set is not available).  The queue size ef (and the Bloom filter size)
-is the smallest point of a sweep whose recall@10 against exact GPU
-brute-force ground truth reaches 0.95.
+evaluation queries from the same mixture, NSW graph with BLOCK_SIZE 32
+(degree 31), k = 10.  Synthetic, seeded stand-in for SIFT1M-shaped data (the
+public set is not available).
+
+Operating points (queue size ef, Bloom size, and the learned form's knobs)
+are chosen on 10,000 separate calibration queries (another seed) as the
+fastest point whose calibration recall@10 reaches 0.95 plus a small margin;
+the numbers reported are those of the 10,000 evaluation queries at that
+point.  Recall is against exact GPU brute-force ground truth.
 
 Two forms are measured.  The plain form is bit-exact with the reference
-search.  The learned form keeps BF16 rows (exact for these integer vectors)
-and uses the learned entry and stop models, trained on the GPU from traces of
-50,000 held-out queries searched by the plain form; its stop threshold is the
-fastest one whose recall@10 reaches 0.95.
+search (kernalGraph.h:184-299).  The learned form adds the tensor-core entry
+stage, the learned entry model and (when it pays) the learned stop, trained
+on the GPU from traces of 50,000 held-out queries searched by the plain form.
+Ablations measure the entry model and the stop model against the same
+search without them.
 
-Outputs one JSON line (rank 0).  ``value`` is device-resident QPS (queries
-and graph already in HBM) of the fastest form meeting the recall target,
-with both forms under ``forms``; ``e2e`` is the same through the host C-ABI
-call (pinned host queries, H2D + kernel + D2H in the timed region).
+The graph: when the reference arm ran first on the same machine it leaves
+the graph the reference's own builder made (build_graph, graph.h:190-199) in
+the cache directory, and this arm searches that graph; otherwise the graph
+comes from the library's GPU builder.  ``config.graph`` says which.
 
-``--impl reference`` times the reference's own CPU search (Graph::search,
-graph.h:33-115, compiled from the reference sources into oracle/_ref) on the
-host cores, at the ef where IT reaches recall@10 0.95 on the same graph.
+Output: ONE compact JSON line on stdout (rank 0; a few KB at most).  Curves,
+sweeps, per-step times and the serving points go to a side file
+(``--details``, default ``gpurun_out/bench_details.json``) and to stderr.
+``value`` is device-resident QPS of the fastest form meeting the recall
+target (queries and graph already in HBM); ``e2e`` is the same through the
+host C-ABI call (pinned host queries, H2D + kernels + D2H timed).
+
+``--impl reference`` runs the reference's own CPU code only (oracle/_ref,
+compiled from the reference sources; none of this library): its graph
+builder, then Graph::search (graph.h:33-115) timed on all host cores and on
+one core (bench_cpu semantics, bench_cpu.cpp:444-451), at the ef where it
+reaches recall@10 0.95 on the same data.
 
 Multi-GPU (torchrun): replicas only -- each rank searches its own 10,000
 queries on its own copy of the graph; no collective on the data path.
@@ -48,18 +62,28 @@ N_BASE = 1_000_000
 DIM = 128
 N_COMP = 1024
 NQ = 10_000
+NCAL = 10_000
 K = 10
 SEED = 2020
+CAL_SEED = SEED + 31337         # calibration queries: same mixture, separate generator
+TRAIN_SEED = SEED + 104729      # training queries of the learned models
 BLOCK_SIZE = 32
 TARGET_RECALL = 0.95
-EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 480, 512, 640, 768, 1024)
+SELECT_MARGIN = 0.002           # points are chosen at calibration recall >= target + margin
+EF_SWEEP = (64, 96, 128, 192, 256, 320, 384, 448, 480, 512, 576, 640, 768, 1024)
 BF_SWEEP = (256, 512, 1024)
+QUEUE_SWEEP = (32, 64, 128, 256)
+EF_SWEEP_K100 = (128, 192, 256, 320, 384, 448, 512, 640, 768, 1024)
 LEARN_THRESHOLDS = (0.8, 0.9, 0.95, 0.98, 1.0)   # 1.0: entry stage alone, no learned stop
 LEARN_EFS = (96, 160)                              # queue sizes the models are trained at
 LEARN_SWEEP_EFS = {96: (64, 72, 80, 88, 96, 128), 160: (160, 192, 256)}
 LEARN_BEAMS = (1, 2, 3, 4)                         # candidates expanded per step
 LEARN_BLOOM_HASHES = (4, 2)                        # BF_NHASH, and the learned search's cheaper test
+ABLATION_EFS = (64, 72, 80, 88, 96, 112, 128, 160, 192, 256, 320, 384, 512)
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
+METRIC = "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or tensor-core entry + learned models)"
+DATA = "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)"
+LINE_LIMIT = 4000                                  # bytes of the stdout JSON line
 
 
 def log(*a):
@@ -85,7 +109,6 @@ class Clocks:
         self.path = os.path.join(tempfile.gettempdir(), f"song_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
@@ -127,19 +150,32 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ------------------------------------------------------------------ workload
+
+def datasets():
+    return importlib.import_module("2020_song_ex_b200.datasets")
+
+
 def make_workload(rank: int):
     """Same base on every rank (replicas); rank r > 0 draws its own queries
     from the same mixture."""
-    ds = importlib.import_module("2020_song_ex_b200.datasets")
+    ds = datasets()
     rep = importlib.import_module("2020_song_ex_b200.replicas")
     m = ds.int_mixture(N_BASE, NQ, dim=DIM, n_comp=N_COMP, seed=SEED,
                        query_seed=rep.query_seed(SEED, rank))
     return m.base, m.queries
 
 
-def build_graph(song, base):
-    return song.build_graph(base, song.Params(block_size=BLOCK_SIZE, fixed_degree=BLOCK_SIZE - 1),
-                            batch_ratio=32)
+def draw_queries(n: int, query_seed: int) -> np.ndarray:
+    """Extra queries from the workload's mixture with their own generator."""
+    return datasets().int_mixture(N_BASE, n, dim=DIM, n_comp=N_COMP, seed=SEED,
+                                  query_seed=query_seed, with_base=False).queries
+
+
+def ref_graph_path() -> str:
+    """Where the reference arm leaves the graph its own builder made."""
+    return os.path.join(datasets().cache_dir(),
+                        f"c2_ref_build_graph_n{N_BASE}_d{DIM}_c{N_COMP}_s{SEED}_bs{BLOCK_SIZE}.song")
 
 
 def peaks():
@@ -185,6 +221,15 @@ def _gpu_index(local: int) -> int:
         except (ValueError, IndexError):
             pass
     return local
+
+
+def choose(points, key="recall_cal"):
+    """Fastest point whose calibration recall reaches the target plus the
+    margin; else the highest-recall point (flagged)."""
+    ok = [p for p in points if p[key] >= TARGET_RECALL + SELECT_MARGIN]
+    if ok:
+        return max(ok, key=lambda p: p["qps"]), True
+    return max(points, key=lambda p: (p[key], p["qps"])), False
 
 
 def timed_device(torch, dist, ws, dev, stream, steps, warmup, launch, clocks_gpu=None, count=None):
@@ -242,296 +287,487 @@ def timed_host(torch, dist, ws, dev, steps, warmup, call):
     return rep.max_over_ranks(dt, device=dev)
 
 
-def run_ours(args, ws, rank, local):
-    import ctypes as C
+def launch_ms(torch, stream, fn, reps=3):
+    """Median CUDA-event time of `reps` launches of fn (one untimed first)."""
+    fn()
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        stream.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return statistics.median(out)
 
+
+# ------------------------------------------------------------------ our arm
+
+class Ctx:
+    """Per-run state shared by the measurement sections."""
+    pass
+
+
+def run_ours(args, ws, rank, local):
     import torch
     import torch.distributed as dist
     song = importlib.import_module("2020_song_ex_b200")
-    ds = importlib.import_module("2020_song_ex_b200.datasets")
+    ds = datasets()
     gtm = importlib.import_module("2020_song_ex_b200.groundtruth")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    L = song.load_library()
+    song.load_library()
+
+    c = Ctx()
+    c.torch, c.dist, c.song, c.ds, c.gtm, c.dev, c.ws, c.rank, c.local, c.args = \
+        torch, dist, song, ds, gtm, dev, ws, rank, local, args
+    details = {}
 
     t0 = time.time()
     base, queries = make_workload(rank)
-    adj = build_graph(song, base)
+    cal = draw_queries(NCAL, CAL_SEED + rank)
+    rp = ref_graph_path()
+    if args.graph in ("auto", "ref") and os.path.exists(rp):
+        adj = ds.load_graph(rp)
+        graph_src = "reference build_graph (graph.h:190-199), made by the reference arm"
+    elif args.graph == "ref":
+        raise SystemExit(f"--graph ref: {rp} not found (run --impl reference first)")
+    else:
+        adj = song.build_graph(base, song.Params(block_size=BLOCK_SIZE, fixed_degree=BLOCK_SIZE - 1),
+                               batch_ratio=32)
+        graph_src = "library GPU builder (batched insertion, ratio 32)"
     torch.cuda.synchronize()
-    build_s = time.time() - t0
-    gt, _ = gtm.knn(base, queries, K)
-    spot = gtm.spot_check(base, queries, gt, sample=16)
+    setup_s = time.time() - t0
+    gt100, _ = gtm.knn(base, queries, 100)
+    gt = np.ascontiguousarray(gt100[:, :K])
+    gt_cal, _ = gtm.knn(base, cal, K)
+    spot = gtm.spot_check(base, queries, gt100, sample=16)
     torch.cuda.empty_cache()
-    log(f"[rank {rank}] workload+graph {build_s:.1f}s, gt spot-check {spot}")
+    log(f"[rank {rank}] workload+graph {setup_s:.1f}s ({graph_src}), gt spot-check {spot}")
+    c.base, c.queries, c.cal, c.adj, c.gt, c.gt100, c.gt_cal = base, queries, cal, adj, gt, gt100, gt_cal
+    c.dq = torch.from_numpy(queries).to(dev)
+    c.dcal = torch.from_numpy(cal).to(dev)
+    c.d_ids = torch.empty((max(NQ, NCAL), K), dtype=torch.int32, device=dev)     # row slices stay contiguous
+    c.d_ids100 = torch.empty((max(NQ, NCAL), 100), dtype=torch.int32, device=dev)
+    c.d_tr = torch.empty((max(NQ, NCAL), 12), dtype=torch.int32, device=dev)
+    c.stream = torch.cuda.Stream(device=dev)
 
-    dq = torch.from_numpy(queries).to(dev)
-    d_ids = torch.empty((NQ, K), dtype=torch.int32, device=dev)
-    d_tr = torch.empty((NQ, 12), dtype=torch.int32, device=dev)
-    stream = torch.cuda.Stream(device=dev)
-
-    # ---------------- plain form: fastest (ef, bf_words) with recall@10 >= 0.95
-    curve, best = [], None
-    graphs = {}
-    sweep = BF_SWEEP if not args.ef else (args.bf_words,)
-    for bfw in sweep:
-        g = song.KernelGraph(N_BASE, DIM, base, song.Params(pq_size=1024, bf_words=bfw), adj=adj)
-        g.upload_to_gpu()
-        graphs[bfw] = g
-        for ef in (EF_SWEEP if not args.ef else (args.ef,)):
-            song.search_device(g, dq, NQ, K, ef, d_ids, d_tr, stream=stream)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream)
-            e1.record(stream)
-            stream.synchronize()
-            ms = e0.elapsed_time(e1)
-            rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
-            pt = {"ef": ef, "bf_words": bfw, "recall": round(rec, 4), "qps": round(NQ / ms * 1e3)}
-            curve.append(pt)
-            if (rec >= TARGET_RECALL or args.ef) and (best is None or pt["qps"] > best["qps"]):
-                best = pt
-            if rec >= TARGET_RECALL:
-                break
-    if best is None:  # not reached: report the highest-recall point
-        best = max(curve, key=lambda p: (p["recall"], p["qps"]))
-    for bfw, g in graphs.items():
-        if bfw != best["bf_words"]:
-            g.close()
-    g = graphs[best["bf_words"]]
-    ef = best["ef"]
-    log(f"[rank {rank}] plain operating point {best}")
-
-    song.search_device(g, dq, NQ, K, ef, d_ids, d_tr, stream=stream)
-    stream.synchronize()
-    trace = d_tr.cpu().numpy()
-    ids_op = d_ids.cpu().numpy()
-    recall = float(ds.recall_at_k(ids_op, gt, K).mean())
-    row_bytes = g.u8_rows() or DIM * 4  # the bench vectors and queries are integers in [0, 255]
-    launch_bytes = float(bytes_per_query(trace, K, row_bytes).sum())
-
-    parity = None
-    if rank == 0 and not args.no_parity:  # bit-exactness at full size (oracle = checker)
-        import oracle
-        sample = 64
-        oids, otr = oracle.search_l2(base, adj, BLOCK_SIZE, queries[:sample], K, ef, pq_size=1024,
-                                     bf_words=best["bf_words"])
-        parity = bool((oids == ids_op[:sample]).all() and (otr == trace[:sample]).all())
-
-    plain_ms, plain_kern, clocks = timed_device(
-        torch, dist, ws, dev, stream, args.steps, args.warmup,
-        lambda: song.search_device(g, dq, NQ, K, ef, d_ids, None, stream=stream),
-        clocks_gpu=_gpu_index(local), count=song.launch_count)
-    plain_launches = timed_device.last_launches
-    plain_qps = ws * NQ * args.steps / (plain_ms / 1e3)
-    if args.no_e2e:
-        g.close()
-        return {"value": round(plain_qps, 1), "note": "profiling case"} if rank == 0 else None
-
-    hq = torch.from_numpy(queries).pin_memory()
-    hids = torch.empty((NQ, K), dtype=torch.int32).pin_memory()
-    hdist = torch.empty((NQ, K), dtype=torch.float32).pin_memory()
-    timing = song._Timing()
-
-    def host_plain():
-        st = L.song_gpu_search(g._h, C.c_void_p(hq.data_ptr()), NQ, K, NQ, ef,
-                               C.c_void_p(hids.data_ptr()), None, C.byref(timing))
-        if st != 0:
-            raise song.SongError(st, L.song_last_error().decode())
-
-    plain_e2e_s = timed_host(torch, dist, ws, dev, args.steps, args.warmup, host_plain)
-    assert np.array_equal(hids.numpy(), ids_op), "host-API ids differ from the device path"
-    plain_e2e = ws * NQ * args.steps / plain_e2e_s
-
-    # ---------------- learned form: BF16 rows + learned entry/stop
-    learned = None
-    if not args.no_learned:
-        ntrain = args.train_queries
-        train = importlib.import_module("2020_song_ex_b200.datasets").int_mixture(
-            N_BASE, ntrain, dim=DIM, n_comp=N_COMP, seed=SEED,
-            query_seed=SEED + 104729 + rank).queries
-        nn1, _ = gtm.knn(base, train, 1)
-        torch.cuda.empty_cache()
-        lcurve, lbest, learn_s, reps, blobs = [], None, 0.0, {}, {}
-        prec = song.PREC_FP32  # the byte rows (exact for these vectors) are read either way
-        for tef in LEARN_EFS:
-            tl0 = time.time()
-            reps[tef] = song.learn(g, torch.from_numpy(train).to(dev), ntrain,
-                                   torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(dev),
-                                   song.LearnParams(k=K, ef=tef))
-            torch.cuda.synchronize()
-            learn_s += time.time() - tl0
-            blobs[tef] = song.get_model(g)
-            # threshold 1.0 (entry model only): every beam and Bloom hash count;
-            # learned stop: beam 1 and 2 with 2 hashes
-            for lef, thr, beam, nh in [(e, t, b, h) for e in LEARN_SWEEP_EFS[tef]
-                                       for t in LEARN_THRESHOLDS
-                                       for b in (LEARN_BEAMS if t >= 1.0 else (1, 2))
-                                       for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))]:
-                    opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam,
-                                           bloom_hashes=nh)
-                    song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
-                    stream.synchronize()  # the ids and traces of this point, not the previous one
-                    rec = float(ds.recall_at_k(d_ids.cpu().numpy(), gt, K).mean())
-                    trl = d_tr.cpu().numpy()
-                    mss = []
-                    for _ in range(3):  # median of three launches
-                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                        e0.record(stream)
-                        song.search_device_ex(g, opts, dq, NQ, K, lef, d_ids, None, None, stream=stream)
-                        e1.record(stream)
-                        stream.synchronize()
-                        mss.append(e0.elapsed_time(e1))
-                    ms = statistics.median(mss)
-                    pt = {"ef": lef, "trained_ef": tef, "threshold": thr, "beam": beam,
-                          "bloom_hashes": nh, "recall": round(rec, 4),
-                          "qps": round(NQ / ms * 1e3),
-                          "mean_expanded": round(float(trl[:, 2].mean()), 1),
-                          "mean_distance_evals": round(float(trl[:, 5].mean()), 1),
-                          "learned_stop_rate": round(float((trl[:, 11] == 2).mean()), 3)}
-                    lcurve.append(pt)
-                    if rec >= TARGET_RECALL and (lbest is None or pt["qps"] > lbest["qps"]):
-                        lbest = pt
-        if lbest is not None:
-            lef = lbest["ef"]
-            song.set_model(g, blobs[lbest["trained_ef"]])
-            rep = reps[lbest["trained_ef"]]
-            lprec = prec
-            lopts = song.SearchOpts(precision=lprec, learned=True, stop_threshold=lbest["threshold"],
-                                    beam=lbest["beam"], bloom_hashes=lbest["bloom_hashes"])
-            lms, lkern, _ = timed_device(
-                torch, dist, ws, dev, stream, args.steps, args.warmup,
-                lambda: song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, None,
-                                              stream=stream), count=song.launch_count)
-            l_launches = timed_device.last_launches
-            ids_l = d_ids.cpu().numpy()
-            song.search_device_ex(g, lopts, dq, NQ, K, lef, d_ids, None, d_tr, stream=stream)
-            stream.synchronize()
-            # gathered rows + the entry stage's hub tiles (hubs x dim BF16 per 128 queries)
-            l_bytes = float(bytes_per_query(d_tr.cpu().numpy(), K, row_bytes).sum()) + \
-                (NQ + 127) // 128 * int(rep.get("n_hubs", 0) or 0) * DIM * 2
-            copts = lopts._c()
-
-            def host_learned():
-                st = L.song_gpu_search_ex(g._h, C.byref(copts), C.c_void_p(hq.data_ptr()), NQ, K,
-                                          NQ, lef, C.c_void_p(hids.data_ptr()),
-                                          C.c_void_p(hdist.data_ptr()), None, C.byref(timing))
-                if st != 0:
-                    raise song.SongError(st, L.song_last_error().decode())
-
-            l_e2e_s = timed_host(torch, dist, ws, dev, args.steps, args.warmup, host_learned)
-            learned = {
-                "form": f"tensor-core entry stage ({int(rep.get('n_hubs', 0) or 0)} hubs) + learned entry/stop model, byte rows",
-                "precision": "u8 rows (exact for these integer vectors)" if row_bytes < DIM * 4 else "fp32",
-                "threshold": lbest["threshold"], "beam": lbest["beam"],
-                "bloom_hashes": lbest["bloom_hashes"], "ef": lef,
-                "trained_ef": lbest["trained_ef"],
-                "qps": round(ws * NQ * args.steps / (lms / 1e3), 1),
-                "e2e_qps": round(ws * NQ * args.steps / l_e2e_s, 1),
-                "recall_at_10": round(float(ds.recall_at_k(ids_l, gt, K).mean()), 4),
-                "ms_per_step": round(lms / args.steps, 4), "gpu_launches": int(l_launches),
-                "algorithmic_bytes_per_launch": round(l_bytes),
-                "kernel_ms_avg": round(statistics.mean(lkern), 4),
-                "kernel_ms": [round(x, 3) for x in lkern],
-                "curve": lcurve, "learn_s": round(learn_s, 2), "train_queries": ntrain,
-                "learn_report": {k2: (round(v, 5) if isinstance(v, float) else v)
-                                 for k2, v in rep.items()},
-            }
-        else:
-            learned = {"curve": lcurve, "note": "no threshold reached recall 0.95",
-                       "learn_report": reps}
-        log(f"[rank {rank}] learned form {lbest}")
-
-    # ---------------- serving: Poisson arrivals, mixed k / queue size, p50/p99 latency
-    serving = None
-    if not args.no_serving:
-        serving = run_serving(song, ds, gtm, torch, g, base, queries, dev, args, rank)
+    plain = measure_plain(c, details)
+    c.g = plain.pop("_graph")
+    queue = measure_queue_sweep(c, details, plain["bf_words"]) if not args.no_queue_sweep else None
+    learned = None if args.no_learned else measure_learned(c, details, plain)
+    serving = None if args.no_serving else measure_serving(c, details)
+    c.g.close()
 
     out = None
     if rank == 0:
         peak, peak_kind = peaks()
-        avg_kern_s = statistics.mean(plain_kern) / 1e3
-        achieved = launch_bytes / avg_kern_s / 1e9
-        traffic, traffic_src = ncu_traffic(ef, best["bf_words"])
-        roof_plain = {
-            "kernel": "plain search_kernel<0,4,1,0,0,0> (bit-exact form)",
-            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-            "traffic": traffic, "traffic_source": traffic_src,
-            "algorithmic_bytes_per_launch": round(launch_bytes),
-            "kernel_ms_avg": round(avg_kern_s * 1e3, 4),
-        }
-        cpu = None if args.no_cpu_baseline else cpu_baseline(base, adj, queries, gt, ef)
-        refgpu = None if args.no_ref_gpu else reference_gpu(base, adj, queries, gt, ef,
-                                                            best["bf_words"], ids_op)
-        use_learned = learned is not None and "qps" in learned and learned["qps"] > plain_qps
+        roof_plain = roofline(plain, peak, peak_kind, "plain search_kernel (bit-exact form)",
+                              ncu_traffic(plain["ef"], plain["bf_words"]))
+        cpu = None if args.no_cpu_baseline else cpu_baseline(base, adj, queries, gt, plain["ef"])
+        refgpu = None if args.no_ref_gpu else reference_gpu(base, adj, queries, plain["ef"],
+                                                            plain["bf_words"], plain["_ids"])
+        use_learned = learned is not None and "qps" in learned and learned["qps"] > plain["qps"]
         roof_learned = None
         if learned is not None and "qps" in learned:
-            la = learned["algorithmic_bytes_per_launch"] / (learned["kernel_ms_avg"] / 1e3) / 1e9
-            lt, lsrc = ncu_traffic(learned["ef"], best["bf_words"], form="learned")
-            roof_learned = {
-                "kernel": ("entry_kernel + search_kernel<0,4,1,0,3,0> (entry model; the stop cannot fire)"
-                           if learned["threshold"] >= 1.0 else
-                           "entry_kernel + search_kernel<0,4,1,0,2,0> (entry + stop models)"),
-                "bound": "hbm", "achieved": round(la, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(la / peak, 4), "peak_kind": peak_kind,
-                "traffic": lt, "traffic_source": lsrc,
-                "algorithmic_bytes_per_launch": learned["algorithmic_bytes_per_launch"],
-                "kernel_ms_avg": learned["kernel_ms_avg"],
-            }
-        value = learned["qps"] if use_learned else plain_qps
-        e2e_v = learned["e2e_qps"] if use_learned else plain_e2e
+            roof_learned = roofline(learned, peak, peak_kind, learned["kernels"],
+                                    ncu_traffic(learned["ef"], plain["bf_words"], form="learned"))
+        best = learned if use_learned else plain
+        details.update({"plain": strip(plain), "learned": strip(learned), "queue_sweep": queue,
+                        "serving": serving, "cpu_baseline": cpu, "reference_gpu_kernel": refgpu,
+                        "roofline_plain": roof_plain, "roofline_learned": roof_learned,
+                        "gt_fp64_spot_check": {"queries": spot[0], "ids_missed": spot[1]},
+                        "graph": graph_src, "setup_s": round(setup_s, 2)})
         out = {
-            "metric": "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or tensor-core entry + learned stop)",
-            "value": round(value, 1),
+            "metric": METRIC,
+            "value": round(best["qps"], 1),
             "unit": "queries/s",
             "n_gpus": ws,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": round((learned["ms_per_step"] if use_learned else plain_ms / args.steps), 4),
+            "ms_per_step": best["ms_per_step"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "u8" if row_bytes < DIM * 4 else "f32",
-            "data": "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)",
+            "dtype": "f32",
+            "data": DATA,
             "config": {
                 "workload": WORKLOAD, "n": N_BASE, "dim": DIM, "nq_per_gpu": NQ, "k": K,
                 "form": "learned" if use_learned else "plain",
-                "ef": learned["ef"] if use_learned else ef, "bf_words": best["bf_words"],
-                "bloom_hashes": learned["bloom_hashes"] if use_learned else 4,
-                "beam": learned["beam"] if use_learned else 1, "pq_size": 1024,
-                "graph": "GPU batched-insertion NSW (ratio 32)",
+                "ef": best["ef"], "bf_words": plain["bf_words"],
+                "bloom_hashes": best.get("bloom_hashes", 4), "beam": best.get("beam", 1),
+                "graph": graph_src,
+                "storage": "u8 byte rows (base is integer 0-255)" if plain["row_bytes"] < DIM * 4
+                           else "fp32 rows",
+                "arithmetic": "exact integer distances equal to the reference's FP32 values",
+                "selection": f"fastest point with recall@10 >= {TARGET_RECALL}+{SELECT_MARGIN} on "
+                             f"{NCAL} calibration queries; reported on the {NQ} evaluation queries",
                 "l2": "inputs larger than L2 (data 512 MB + adj 128 MB per GPU)",
                 "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
             },
-            "recall_at_10": learned["recall_at_10"] if use_learned else round(recall, 4),
-            "forms": {
-                "plain": {"qps": round(plain_qps, 1), "e2e_qps": round(plain_e2e, 1),
-                          "recall_at_10": round(recall, 4), "operating_point": best,
-                          "ms_per_step": round(plain_ms / args.steps, 4),
-                          "gpu_launches": int(plain_launches),
-                          "parity_sample_bit_exact": parity},
-                "learned": learned,
-                "learned_over_plain": (round(learned["qps"] / plain_qps, 3)
-                                       if learned and "qps" in learned else None),
-            },
-            "recall_curve": curve,
-            "gt_fp64_spot_check": {"queries": spot[0], "ids_missed": spot[1]},
-            "e2e": {"value": round(e2e_v, 1), "unit": "queries/s",
+            "recall_at_10": best["recall_at_10"],
+            "e2e": {"value": round(best["e2e_qps"], 1), "unit": "queries/s",
                     "h2d_bytes_per_step": int(queries.nbytes),
                     "d2h_bytes_per_step": int(NQ * K * (8 if use_learned else 4))},
-            "gpu_launches": int(learned["gpu_launches"] if use_learned else plain_launches),
+            "gpu_launches": int(best["gpu_launches"]),
             "roofline": roof_learned if use_learned else roof_plain,
             "roofline_plain": roof_plain,
-            "serving": serving,
             "cpu_baseline": cpu,
-            "reference_gpu_kernel": refgpu,
-            "clocks": clocks,
-            "trace_means": {k2: round(float(v), 2) for k2, v in
-                            zip(song.TRACE_FIELDS, trace.mean(axis=0))},
-            "build_s": round(build_s, 2),
+            "clocks": plain["clocks"],
+            "forms": {"plain": summary_plain(plain),
+                      "learned": summary_learned(learned),
+                      "learned_over_plain": (round(learned["qps"] / plain["qps"], 3)
+                                             if learned and "qps" in learned else None)},
+            "configs": {"c2_queue_sweep": summary_queue(queue), "c5_serving": summary_serving(serving)},
+            "reference_gpu_kernel": ({"qps": refgpu.get("qps_total"),
+                                      "ids_identical": refgpu.get("ids_identical_to_ours")}
+                                     if refgpu and "qps_total" in refgpu else refgpu),
         }
-    g.close()
-    return out
+        if args.configs:
+            ex = measure_extra_configs(c, details, args.configs.split(","))
+            out["configs"].update(ex)
+    return out, details
+
+
+def strip(d):
+    if d is None:
+        return None
+    return {k: v for k, v in d.items() if not k.startswith("_")}
+
+
+def roofline(form, peak, peak_kind, kernel, traffic_src):
+    achieved = form["algorithmic_bytes_per_launch"] / (form["kernel_ms_avg"] / 1e3) / 1e9
+    traffic, src = traffic_src
+    return {"kernel": kernel, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": traffic, "traffic_source": src,
+            "algorithmic_bytes_per_launch": form["algorithmic_bytes_per_launch"],
+            "kernel_ms_avg": form["kernel_ms_avg"]}
+
+
+def measure_plain(c, details):
+    """The plain bit-exact form: (ef, bf_words) chosen on calibration queries,
+    then timed and checked on the evaluation queries."""
+    torch, song, ds, args = c.torch, c.song, c.ds, c.args
+    import ctypes as C
+    L = song.load_library()
+    stream, d_ids, d_tr = c.stream, c.d_ids, c.d_tr
+    curve, graphs = [], {}
+    bfs = BF_SWEEP if not args.ef else (args.bf_words,)
+    efs = EF_SWEEP if not args.ef else (args.ef,)
+    for bfw in bfs:
+        g = song.KernelGraph(N_BASE, DIM, c.base, song.Params(pq_size=1024, bf_words=bfw), adj=c.adj)
+        g.upload_to_gpu()
+        graphs[bfw] = g
+        for ef in efs:
+            ids_v = d_ids[:NCAL]
+            ms = launch_ms(torch, stream, lambda: song.search_device(g, c.dcal, NCAL, K, ef, ids_v, None,
+                                                                     stream=stream), reps=1)
+            rec = float(ds.recall_at_k(ids_v.cpu().numpy(), c.gt_cal, K).mean())
+            curve.append({"ef": ef, "bf_words": bfw, "recall_cal": round(rec, 4),
+                          "qps": round(NCAL / ms * 1e3)})
+            if rec >= TARGET_RECALL + SELECT_MARGIN:
+                break
+    op, reached = choose(curve) if not args.ef else (curve[0], True)
+    for bfw, g in graphs.items():
+        if bfw != op["bf_words"]:
+            g.close()
+    g = graphs[op["bf_words"]]
+    ef = op["ef"]
+    log(f"[rank {c.rank}] plain operating point {op}")
+    ids_v = d_ids[:NQ]
+    song.search_device(g, c.dq, NQ, K, ef, ids_v, d_tr[:NQ], stream=stream)
+    stream.synchronize()
+    trace = d_tr[:NQ].cpu().numpy()
+    ids_op = ids_v.cpu().numpy()
+    recall = float(ds.recall_at_k(ids_op, c.gt, K).mean())
+    row_bytes = g.u8_rows() or DIM * 4  # the bench vectors and queries are integers in [0, 255]
+    launch_bytes = float(bytes_per_query(trace, K, row_bytes).sum())
+    parity = None
+    if c.rank == 0 and not args.no_parity:  # bit-exactness at full size (oracle = checker)
+        import oracle
+        sample = 64
+        oids, otr = oracle.search_l2(c.base, c.adj, BLOCK_SIZE, c.queries[:sample], K, ef,
+                                     pq_size=1024, bf_words=op["bf_words"])
+        parity = bool((oids == ids_op[:sample]).all() and (otr == trace[:sample]).all())
+    total_ms, kern, clocks = timed_device(
+        torch, c.dist, c.ws, c.dev, stream, args.steps, args.warmup,
+        lambda: song.search_device(g, c.dq, NQ, K, ef, ids_v, None, stream=stream),
+        clocks_gpu=_gpu_index(c.local), count=song.launch_count)
+    launches = timed_device.last_launches
+    qps = c.ws * NQ * args.steps / (total_ms / 1e3)
+    e2e = None
+    if not args.no_e2e:
+        hq = torch.from_numpy(c.queries).pin_memory()
+        hids = torch.empty((NQ, K), dtype=torch.int32).pin_memory()
+        timing = song._Timing()
+
+        def host_plain():
+            st = L.song_gpu_search(g._h, C.c_void_p(hq.data_ptr()), NQ, K, NQ, ef,
+                                   C.c_void_p(hids.data_ptr()), None, C.byref(timing))
+            if st != 0:
+                raise song.SongError(st, L.song_last_error().decode())
+
+        e2e_s = timed_host(torch, c.dist, c.ws, c.dev, args.steps, args.warmup, host_plain)
+        assert np.array_equal(hids.numpy(), ids_op), "host-API ids differ from the device path"
+        e2e = c.ws * NQ * args.steps / e2e_s
+    details["plain_curve"] = curve
+    details["plain_kernel_ms"] = [round(x, 3) for x in kern]
+    details["plain_trace_means"] = {k2: round(float(v), 2) for k2, v in
+                                    zip(song.TRACE_FIELDS, trace.mean(axis=0))}
+    return {"_graph": g, "_ids": ids_op, "ef": ef, "bf_words": op["bf_words"],
+            "reached_on_calibration": reached, "recall_cal": op["recall_cal"],
+            "qps": qps, "e2e_qps": e2e if e2e is not None else qps,
+            "recall_at_10": round(recall, 4), "ms_per_step": round(total_ms / args.steps, 4),
+            "gpu_launches": int(launches), "algorithmic_bytes_per_launch": round(launch_bytes),
+            "kernel_ms_avg": round(statistics.mean(kern), 4), "row_bytes": row_bytes,
+            "parity_sample_bit_exact": parity, "clocks": clocks,
+            "mean_expanded": round(float(trace[:, 2].mean()), 1),
+            "mean_distance_evals": round(float(trace[:, 5].mean()), 1)}
+
+
+def measure_queue_sweep(c, details, bf_words):
+    """Plain form at queue sizes 32..256 for k = 10 and k = 100 (recall@k on
+    the evaluation queries), and the k = 100 operating point for recall@100
+    >= 0.95 (chosen on calibration queries)."""
+    torch, song, ds = c.torch, c.song, c.ds
+    g = c.g
+    stream = c.stream
+    pts = []
+    for k in (10, 100):
+        gtk = c.gt100[:, :k]
+        for ef in QUEUE_SWEEP:
+            ids_v = (c.d_ids if k == K else c.d_ids100)[:NQ]
+            ms = launch_ms(torch, stream, lambda: song.search_device(g, c.dq, NQ, k, ef, ids_v, None,
+                                                                     stream=stream))
+            rec = float(ds.recall_at_k(ids_v.cpu().numpy(), gtk, k).mean())
+            pts.append({"k": k, "ef": ef, "ef_effective": min(max(ef, k), 1024),
+                        f"recall@{k}": round(rec, 4), "qps": round(NQ / ms * 1e3)})
+    # k = 100: calibration sweep for recall@100 >= target
+    gt_cal100, _ = c.gtm.knn(c.base, c.cal, 100)
+    cal_pts = []
+    for ef in EF_SWEEP_K100:
+        ids_v = c.d_ids100[:NCAL]
+        ms = launch_ms(torch, stream, lambda: song.search_device(g, c.dcal, NCAL, 100, ef, ids_v, None,
+                                                                 stream=stream), reps=1)
+        rec = float(ds.recall_at_k(ids_v.cpu().numpy(), gt_cal100, 100).mean())
+        cal_pts.append({"ef": ef, "recall_cal": round(rec, 4), "qps": round(NCAL / ms * 1e3)})
+        if rec >= TARGET_RECALL + SELECT_MARGIN:
+            break
+    op, reached = choose(cal_pts)
+    ids_v = c.d_ids100[:NQ]
+    ms = launch_ms(torch, stream, lambda: song.search_device(g, c.dq, NQ, 100, op["ef"], ids_v, None,
+                                                             stream=stream), reps=5)
+    rec = float(ds.recall_at_k(ids_v.cpu().numpy(), c.gt100, 100).mean())
+    k100 = {"ef": op["ef"], "qps": round(NQ / ms * 1e3), "recall@100": round(rec, 4),
+            "reached_on_calibration": reached}
+    details["queue_sweep"] = pts
+    details["k100_calibration_curve"] = cal_pts
+    log(f"[rank {c.rank}] k=100 operating point {k100}")
+    return {"points": pts, "k100": k100, "bf_words": bf_words}
+
+
+def summary_queue(q):
+    if q is None:
+        return None
+    s = {f"k{p['k']}_ef{p['ef']}": [p["qps"], p[f"recall@{p['k']}"]] for p in q["points"]}
+    s["k100_at_0.95"] = {"qps": q["k100"]["qps"], "ef": q["k100"]["ef"],
+                         "recall@100": q["k100"]["recall@100"]}
+    s["cols"] = "qps, recall@k (eval queries)"
+    return s
+
+
+def measure_learned(c, details, plain):
+    """Learned form: models trained on 50,000 held-out queries; the knobs are
+    chosen on calibration queries; then timed, and ablated, on the
+    evaluation queries."""
+    torch, song, ds, gtm, args = c.torch, c.song, c.ds, c.gtm, c.args
+    import ctypes as C
+    L = song.load_library()
+    g, stream, dev = c.g, c.stream, c.dev
+    ntrain = args.train_queries
+    train = draw_queries(ntrain, TRAIN_SEED + c.rank)
+    nn1, _ = gtm.knn(c.base, train, 1)
+    torch.cuda.empty_cache()
+    ids_cal = c.d_ids[:NCAL]
+    ids_ev = c.d_ids[:NQ]
+    tr_cal = c.d_tr[:NCAL]
+    lcurve, reps, blobs, learn_s = [], {}, {}, 0.0
+    prec = song.PREC_FP32  # the byte rows (exact for these vectors) are read either way
+    for tef in LEARN_EFS:
+        tl0 = time.time()
+        reps[tef] = song.learn(g, torch.from_numpy(train).to(dev), ntrain,
+                               torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(dev),
+                               song.LearnParams(k=K, ef=tef))
+        torch.cuda.synchronize()
+        learn_s += time.time() - tl0
+        blobs[tef] = song.get_model(g)
+        # threshold 1.0 (entry model only): every beam and Bloom hash count;
+        # learned stop: beam 1 and 2 with 2 hashes
+        for lef, thr, beam, nh in [(e, t, b, h) for e in LEARN_SWEEP_EFS[tef]
+                                   for t in LEARN_THRESHOLDS
+                                   for b in (LEARN_BEAMS if t >= 1.0 else (1, 2))
+                                   for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))]:
+            opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam,
+                                   bloom_hashes=nh)
+            song.search_device_ex(g, opts, c.dcal, NCAL, K, lef, ids_cal, None, tr_cal, stream=stream)
+            stream.synchronize()
+            rec = float(ds.recall_at_k(ids_cal.cpu().numpy(), c.gt_cal, K).mean())
+            trl = tr_cal.cpu().numpy()
+            ms = launch_ms(torch, stream, lambda: song.search_device_ex(
+                g, opts, c.dcal, NCAL, K, lef, ids_cal, None, None, stream=stream))
+            lcurve.append({"ef": lef, "trained_ef": tef, "threshold": thr, "beam": beam,
+                           "bloom_hashes": nh, "recall_cal": round(rec, 4),
+                           "qps": round(NCAL / ms * 1e3),
+                           "mean_expanded": round(float(trl[:, 2].mean()), 1),
+                           "learned_stop_rate": round(float((trl[:, 11] == 2).mean()), 3)})
+    details["learned_curve"] = lcurve
+    details["learn_reports"] = {str(t): {k2: (round(v, 5) if isinstance(v, float) else v)
+                                         for k2, v in r.items()} for t, r in reps.items()}
+    op, reached = choose(lcurve)
+    stop_pts = [p for p in lcurve if p["threshold"] < 1.0]
+    nostop_pts = [p for p in lcurve if p["threshold"] >= 1.0]
+    log(f"[rank {c.rank}] learned operating point {op}")
+
+    def opts_of(p, entry=song.ENTRY_MODEL):
+        return song.SearchOpts(precision=prec, learned=True, stop_threshold=p["threshold"],
+                               beam=p["beam"], bloom_hashes=p["bloom_hashes"], entry=entry)
+
+    def evaluate(p, entry=song.ENTRY_MODEL, reps_=5):
+        """Recall, QPS and trace means of point p on the evaluation queries."""
+        song.set_model(g, blobs[p["trained_ef"]])
+        o = opts_of(p, entry)
+        song.search_device_ex(g, o, c.dq, NQ, K, p["ef"], ids_ev, None, c.d_tr[:NQ], stream=stream)
+        stream.synchronize()
+        rec = float(ds.recall_at_k(ids_ev.cpu().numpy(), c.gt, K).mean())
+        tr = c.d_tr[:NQ].cpu().numpy()
+        ms = launch_ms(torch, stream, lambda: song.search_device_ex(
+            g, o, c.dq, NQ, K, p["ef"], ids_ev, None, None, stream=stream), reps=reps_)
+        return {"ef": p["ef"], "trained_ef": p["trained_ef"], "threshold": p["threshold"],
+                "beam": p["beam"], "bloom_hashes": p["bloom_hashes"], "recall_at_10": round(rec, 4),
+                "qps": round(NQ / ms * 1e3), "mean_expanded": round(float(tr[:, 2].mean()), 1),
+                "learned_stop_rate": round(float((tr[:, 11] == 2).mean()), 3)}, tr
+
+    def ablate(entry):
+        """The op point's knobs with another entry choice, ef re-chosen on the
+        calibration queries for the same recall target, evaluated."""
+        song.set_model(g, blobs[op["trained_ef"]])
+        pts = []
+        for ef in ABLATION_EFS:
+            p = dict(op, ef=ef)
+            o = opts_of(p, entry)
+            song.search_device_ex(g, o, c.dcal, NCAL, K, ef, ids_cal, None, None, stream=stream)
+            stream.synchronize()
+            rec = float(ds.recall_at_k(ids_cal.cpu().numpy(), c.gt_cal, K).mean())
+            ms = launch_ms(torch, stream, lambda: song.search_device_ex(
+                g, o, c.dcal, NCAL, K, ef, ids_cal, None, None, stream=stream), reps=1)
+            pts.append(dict(p, recall_cal=round(rec, 4), qps=round(NCAL / ms * 1e3)))
+            if rec >= TARGET_RECALL + SELECT_MARGIN:
+                break
+        best, ok = choose(pts)
+        ev, _ = evaluate(best, entry)
+        ev["reached_on_calibration"] = ok
+        same_ef, _ = evaluate(op, entry, reps_=3)
+        return {"at_target": ev, "at_op_ef": {"ef": op["ef"], "recall_at_10": same_ef["recall_at_10"],
+                                              "qps": same_ef["qps"]}}
+
+    ablation = {"no_entry_model": ablate(song.ENTRY_NEAREST),
+                "reference_seeds": ablate(song.ENTRY_SEEDS)}
+    if stop_pts and nostop_pts:
+        bs, oks = choose(stop_pts)
+        bn, okn = choose(nostop_pts)
+        es, _ = evaluate(bs)
+        en, _ = evaluate(bn)
+        es["reached_on_calibration"], en["reached_on_calibration"] = oks, okn
+        ablation["stop_model_on"] = es
+        ablation["stop_model_off"] = en
+    details["learned_ablation"] = ablation
+
+    # the operating point, timed on the evaluation queries
+    song.set_model(g, blobs[op["trained_ef"]])
+    lopts = opts_of(op)
+    lef = op["ef"]
+    total_ms, kern, _ = timed_device(
+        torch, c.dist, c.ws, dev, stream, args.steps, args.warmup,
+        lambda: song.search_device_ex(g, lopts, c.dq, NQ, K, lef, ids_ev, None, None, stream=stream),
+        count=song.launch_count)
+    launches = timed_device.last_launches
+    ids_l = ids_ev.cpu().numpy()
+    song.search_device_ex(g, lopts, c.dq, NQ, K, lef, ids_ev, None, c.d_tr[:NQ], stream=stream)
+    stream.synchronize()
+    tr = c.d_tr[:NQ].cpu().numpy()
+    rep = reps[op["trained_ef"]]
+    n_hubs = int(rep.get("n_hubs", 0) or 0)
+    # gathered rows + the entry stage's hub tiles (hubs x dim BF16 per 128 queries)
+    l_bytes = float(bytes_per_query(tr, K, plain["row_bytes"]).sum()) + \
+        (NQ + 127) // 128 * n_hubs * DIM * 2
+    e2e = None
+    if not args.no_e2e:
+        hq = torch.from_numpy(c.queries).pin_memory()
+        hids = torch.empty((NQ, K), dtype=torch.int32).pin_memory()
+        hdist = torch.empty((NQ, K), dtype=torch.float32).pin_memory()
+        timing = song._Timing()
+        copts = lopts._c()
+
+        def host_learned():
+            st = L.song_gpu_search_ex(g._h, C.byref(copts), C.c_void_p(hq.data_ptr()), NQ, K,
+                                      NQ, lef, C.c_void_p(hids.data_ptr()),
+                                      C.c_void_p(hdist.data_ptr()), None, C.byref(timing))
+            if st != 0:
+                raise song.SongError(st, L.song_last_error().decode())
+
+        e2e = c.ws * NQ * args.steps / timed_host(torch, c.dist, c.ws, dev, args.steps, args.warmup,
+                                                  host_learned)
+    details["learned_kernel_ms"] = [round(x, 3) for x in kern]
+    return {
+        "form": f"tensor-core entry stage ({n_hubs} hubs) + learned entry model"
+                + (" + learned stop" if op["threshold"] < 1.0 else "") + ", byte rows",
+        "kernels": ("entry_kernel + search_kernel<0,4,1,0,3,0> (entry model; the stop cannot fire)"
+                    if op["threshold"] >= 1.0 else
+                    "entry_kernel + search_kernel<0,4,1,0,2,0> (entry + stop models)"),
+        "threshold": op["threshold"], "beam": op["beam"], "bloom_hashes": op["bloom_hashes"],
+        "ef": lef, "trained_ef": op["trained_ef"], "recall_cal": op["recall_cal"],
+        "reached_on_calibration": reached,
+        "qps": c.ws * NQ * args.steps / (total_ms / 1e3),
+        "e2e_qps": e2e if e2e is not None else c.ws * NQ * args.steps / (total_ms / 1e3),
+        "recall_at_10": round(float(ds.recall_at_k(ids_l, c.gt, K).mean()), 4),
+        "ms_per_step": round(total_ms / args.steps, 4), "gpu_launches": int(launches),
+        "algorithmic_bytes_per_launch": round(l_bytes),
+        "kernel_ms_avg": round(statistics.mean(kern), 4),
+        "mean_expanded": round(float(tr[:, 2].mean()), 1),
+        "learned_stop_rate": round(float((tr[:, 11] == 2).mean()), 3),
+        "learn_s": round(learn_s, 2), "train_queries": ntrain, "ablation": ablation,
+    }
+
+
+def summary_plain(p):
+    return {"qps": round(p["qps"], 1), "e2e_qps": round(p["e2e_qps"], 1),
+            "recall_at_10": p["recall_at_10"], "ef": p["ef"], "bf_words": p["bf_words"],
+            "bit_exact_sample": p["parity_sample_bit_exact"],
+            "mean_expanded": p["mean_expanded"]}
+
+
+def summary_learned(l):
+    if l is None or "qps" not in l:
+        return l
+    ab = l.get("ablation", {})
+
+    def short(e):
+        if e is None:
+            return None
+        e = e.get("at_target", e)
+        return [e["qps"], e["recall_at_10"], e["ef"]]
+
+    return {"qps": round(l["qps"], 1), "e2e_qps": round(l["e2e_qps"], 1),
+            "recall_at_10": l["recall_at_10"], "ef": l["ef"], "beam": l["beam"],
+            "bloom_hashes": l["bloom_hashes"], "stop_threshold": l["threshold"],
+            "learned_stop_rate": l["learned_stop_rate"], "mean_expanded": l["mean_expanded"],
+            "ablation_qps_recall_ef": {
+                "entry_model": [round(l["qps"]), l["recall_at_10"], l["ef"]],
+                "no_entry_model": short(ab.get("no_entry_model")),
+                "reference_seeds": short(ab.get("reference_seeds")),
+                "stop_model_on": short(ab.get("stop_model_on")),
+                "stop_model_off": short(ab.get("stop_model_off"))}}
 
 
 SERVE_KS = (1, 10, 100)
@@ -539,46 +775,71 @@ SERVE_EFS = (32, 64, 128, 256)
 SERVE_RATES = (5_000, 20_000, 50_000, 100_000, 200_000)
 
 
-def run_serving(song, ds, gtm, torch, g, base, queries, dev, args, rank):
+def measure_serving(c, details):
     """Continuous-batching server over the same index: Poisson arrivals at
     several rates, k ~ U{1,10,100}, queue ~ U{32,...,256}; every request uses
     the learned entry/stop (trained here at queue 256, k 10) and falls back to
     the full search when not confident.  Per rate: achieved QPS, p50/p99
-    latency (arrival to completion seen by the host), recall@k per k."""
+    latency (arrival to completion seen by the host), recall@k per k and per
+    queue size."""
+    torch, song, ds, gtm, args = c.torch, c.song, c.ds, c.gtm, c.args
+    g = c.g
     ntrain = min(args.train_queries, 20_000)
-    train = ds.int_mixture(N_BASE, ntrain, dim=DIM, n_comp=N_COMP, seed=SEED,
-                           query_seed=SEED + 7 * 104729 + rank).queries
-    nn1, _ = gtm.knn(base, train, 1)
-    gt100, _ = gtm.knn(base, queries, 100)
+    train = draw_queries(ntrain, SEED + 7 * 104729 + c.rank)
+    nn1, _ = gtm.knn(c.base, train, 1)
     torch.cuda.empty_cache()
-    song.learn(g, torch.from_numpy(train).to(dev), ntrain,
-               torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(dev),
+    song.learn(g, torch.from_numpy(train).to(c.dev), ntrain,
+               torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(c.dev),
                song.LearnParams(k=10, ef=max(SERVE_EFS)))
-    rng = np.random.default_rng(SEED + rank)
+    rng = np.random.default_rng(SEED + c.rank)
     out = []
     cfg = song.ServerConfig(max_k=max(SERVE_KS), max_ef=max(SERVE_EFS), stop_threshold=0.85)
     with song.Server(g, cfg) as srv:
         for rate in SERVE_RATES:
-            nreq = int(min(len(queries), max(2000, rate * args.serve_seconds)))
-            idx = rng.integers(0, len(queries), nreq)
+            nreq = int(min(NQ, max(2000, rate * args.serve_seconds)))
+            idx = rng.integers(0, NQ, nreq)
             ks = rng.choice(SERVE_KS, nreq).astype(np.int32)
             efs = rng.choice(SERVE_EFS, nreq).astype(np.int32)
             flags = np.full(nreq, song.REQ_LEARNED, np.int32)
-            lat, ids, wall = srv.run_poisson(queries[idx], ks, efs, flags, float(rate),
-                                             seed=int(rate))
+            lat, ids, wall = srv.run_poisson(c.queries[idx], ks, efs, flags, float(rate), seed=int(rate))
             rec = {}
             for k in SERVE_KS:
                 sel = ks == k
                 if sel.any():
-                    rec[f"recall@{k}"] = round(float(ds.recall_at_k(ids[sel, :k], gt100[idx[sel], :k], k).mean()), 4)
+                    rec[f"recall@{k}"] = round(float(ds.recall_at_k(ids[sel, :k], c.gt100[idx[sel], :k],
+                                                                     k).mean()), 4)
+            by_ef = {}
+            for ef in SERVE_EFS:  # recall@min(k,10) per queue size: the latency-recall trade
+                sel = efs == ef
+                if sel.any():
+                    kk = np.minimum(ks[sel], 10)
+                    r = [float(ds.recall_at_k(ids[sel][kk == k, :k], c.gt100[idx[sel]][kk == k, :k],
+                                              k).sum()) for k in np.unique(kk)]
+                    by_ef[str(ef)] = {"recall": round(sum(r) / int(sel.sum()), 4),
+                                      "p50_ms": round(float(np.percentile(lat[sel], 50)), 3),
+                                      "p99_ms": round(float(np.percentile(lat[sel], 99)), 3)}
             out.append({"offered_qps": rate, "requests": nreq,
                         "achieved_qps": round(nreq / wall, 1) if wall > 0 else None,
                         "p50_ms": round(float(np.percentile(lat, 50)), 3),
                         "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                        "mean_ms": round(float(lat.mean()), 3), **rec})
-            log(f"[rank {rank}] serving {out[-1]}")
-    return {"form": "FP32 + learned entry/stop (full search when not confident)",
+                        "mean_ms": round(float(lat.mean()), 3), **rec, "by_queue": by_ef})
+            log(f"[rank {c.rank}] serving {out[-1]}")
+    details["serving"] = out
+    return {"form": "learned entry/stop at threshold 0.85, full search when not confident",
             "k_choices": list(SERVE_KS), "queue_choices": list(SERVE_EFS), "points": out}
+
+
+def summary_serving(s):
+    if s is None:
+        return None
+    return {"cols": "offered, achieved qps, p50 ms, p99 ms, recall@10",
+            "points": [[p["offered_qps"], p["achieved_qps"], p["p50_ms"], p["p99_ms"],
+                        p.get("recall@10")] for p in s["points"]]}
+
+
+def measure_extra_configs(c, details, names):
+    """Other workloads (filled in by later sections)."""
+    return {}
 
 
 def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
@@ -589,7 +850,7 @@ def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
     except Exception as e:  # reference not built
         return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
                 "sample": f"unavailable: {e}"}
-    ds = importlib.import_module("2020_song_ex_b200.datasets")
+    ds = datasets()
     threads = os.cpu_count() or 1
     cg = r.cpu_graph(base, adj)
     cg.search(queries[:64], K, ef, threads=threads)  # warm
@@ -600,11 +861,11 @@ def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
     cg.close()
     return {"value": round(sample / dt, 1), "unit": "queries/s", "cores": threads,
             "kind": "reference",
-            "sample": f"{sample} of the {NQ} queries at ef={ef}, Graph::search (graph.h:33) "
+            "sample": f"{sample} eval queries at ef={ef}, Graph::search (graph.h:33) "
                       f"from oracle/_ref on {threads} threads; its recall@10 {rec:.4f}"}
 
 
-def reference_gpu(base, adj, queries, gt, ef, bf_words, ours):
+def reference_gpu(base, adj, queries, ef, bf_words, ours):
     """The reference's own GPU kernel (kg_search_kernel via gpu_search, compiled
     for sm_100a), same graph and parameters: QPS and id agreement."""
     try:
@@ -614,38 +875,91 @@ def reference_gpu(base, adj, queries, gt, ef, bf_words, ours):
             raise FileNotFoundError("libref_gpu.so not built")
     except Exception as e:
         return {"unavailable": str(e)}
-    ids, _tr, timing = r.gpu_search_l2(base, adj, queries, K, ef)  # warm (JIT-free: sm_100a SASS)
+    ids, _tr, timing = r.gpu_search_l2(base, adj, queries, K, ef)  # warm
     ids, _tr, timing = r.gpu_search_l2(base, adj, queries, K, ef)
     return {"qps_total": round(NQ / (timing[4] / 1e3), 1), "kernel_ms": round(timing[2], 3),
             "total_ms": round(timing[4], 3), "ids_identical_to_ours": bool((ids == ours).all()),
             "note": "gpu_search (kernalGraph.h:307) on the same graph: 512-query batches, H2D+kernel+D2H"}
 
 
+# ------------------------------------------------------------------ reference arm
+
+def cpu_info() -> dict:
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.lower().startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return {"model": model, "cores_visible": os.cpu_count(),
+            "cores_usable": len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else None}
+
+
+def exact_knn_cpu(base, queries, k, chunk=512):
+    """Exact top-k on the host with FP32 GEMMs (torch on CPU, all threads).
+    For integer vectors in [0, 255] of dim 128 every term of
+    |q|^2 + |b|^2 - 2 q.b is an integer below 2^24, so the FP32 values are
+    exact; ties go to the lower id."""
+    import torch
+    b = torch.from_numpy(np.ascontiguousarray(base, dtype=np.float32))
+    bn = (b * b).sum(1)
+    out = np.empty((queries.shape[0], k), np.int32)
+    for s in range(0, queries.shape[0], chunk):
+        q = torch.from_numpy(np.ascontiguousarray(queries[s:s + chunk], dtype=np.float32))
+        d = (q * q).sum(1)[:, None] + bn[None, :] - 2.0 * (q @ b.T)
+        v, i = torch.topk(d, k + 8, dim=1, largest=False, sorted=True)
+        v, i = v.numpy(), i.numpy()
+        for r in range(v.shape[0]):  # (distance, id) order among the candidates
+            o = np.lexsort((i[r], v[r]))[:k]
+            out[s + r] = i[r][o]
+    return out
+
+
 def run_reference(args, ws, rank, local):
-    """--impl reference: the reference CPU search on the host cores."""
+    """--impl reference: the reference's own CPU code on the host cores --
+    its graph builder and Graph::search -- and nothing of this library."""
     if rank != 0:
-        return None
-    ds = importlib.import_module("2020_song_ex_b200.datasets")
+        return None, None
+    ds = datasets()
     try:
         import oracle
         r = oracle.ref(block_size=BLOCK_SIZE, bf_words=256, pq_size=512)
     except Exception as e:
-        return {"impl": "reference", "unavailable": f"compiled reference not available: {e}"}
-    song = importlib.import_module("2020_song_ex_b200")
-    gtm = importlib.import_module("2020_song_ex_b200.groundtruth")
+        return {"impl": "reference", "unavailable": f"compiled reference not available: {e}"}, None
     base, queries = make_workload(0)
-    adj = build_graph(song, base)  # setup only (same graph as our arm); untimed
-    gt, _ = gtm.knn(base, queries, K)
-    threads = os.cpu_count() or 1
-    cg = r.cpu_graph(base, adj)
+    cal = draw_queries(NCAL, CAL_SEED)
+    rp = ref_graph_path()
+    t0 = time.time()
+    if os.path.exists(rp):
+        adj = ds.load_graph(rp)
+        build_s = None
+    else:
+        adj = np.empty((N_BASE, BLOCK_SIZE), np.int32)
+        if r.cpu.ref_cpu_build_graph(np.ascontiguousarray(base), N_BASE, DIM, adj) != 0:
+            raise RuntimeError("reference build_graph failed")
+        build_s = round(time.time() - t0, 1)
+        tmp = rp + f".tmp{os.getpid()}"
+        ds.save_graph(tmp, adj)
+        os.replace(tmp, rp)
+    log(f"[reference] graph: build_graph {build_s} s")
+    t1 = time.time()
+    gt = exact_knn_cpu(base, queries, K)
     rng = np.random.default_rng(1)
-    sweep_q = rng.choice(NQ, 400, replace=False)
+    sweep_q = rng.choice(NCAL, 500, replace=False)
+    gt_cal = exact_knn_cpu(base, cal[sweep_q], K)
+    log(f"[reference] exact kNN on the host {time.time() - t1:.1f} s")
+    threads = os.cpu_count() or 1
+    if hasattr(os, "sched_getaffinity"):
+        threads = len(os.sched_getaffinity(0))
+    cg = r.cpu_graph(base, adj)
     ef_op, curve = None, []
     for ef in EF_SWEEP:
-        ids, _ = cg.search(queries[sweep_q], K, ef, threads=threads)
-        rec = float(ds.recall_at_k(ids, gt[sweep_q], K).mean())
-        curve.append({"ef": ef, "recall": round(rec, 4)})
-        if rec >= TARGET_RECALL:
+        ids, _ = cg.search(cal[sweep_q], K, ef, threads=threads)
+        rec = float(ds.recall_at_k(ids, gt_cal, K).mean())
+        curve.append({"ef": ef, "recall_cal": round(rec, 4)})
+        if rec >= TARGET_RECALL + SELECT_MARGIN:
             ef_op = ef
             break
     if ef_op is None:
@@ -654,26 +968,41 @@ def run_reference(args, ws, rank, local):
     times = []
     for i in range(args.warmup + args.steps):
         sel = np.arange(i * per_step, (i + 1) * per_step) % NQ
-        t0 = time.perf_counter()
+        ts = time.perf_counter()
         cg.search(queries[sel], K, ef_op, threads=threads)
         if i >= args.warmup:
-            times.append(time.perf_counter() - t0)
+            times.append(time.perf_counter() - ts)
     total = sum(times)
     qps = per_step * args.steps / total
     ids, _ = cg.search(queries[:per_step], K, ef_op, threads=threads)
     rec = float(ds.recall_at_k(ids, gt[:per_step], K).mean())
+    # bench_cpu semantics: one thread, per-query latency (bench_cpu.cpp:444-451)
+    n1 = args.ref_single_queries
+    lat = []
+    for i in range(n1):
+        ts = time.perf_counter()
+        cg.search(queries[i:i + 1], K, ef_op, threads=1)
+        lat.append(time.perf_counter() - ts)
+    lat = np.array(lat)
+    single = {"qps": round(n1 / lat.sum(), 1), "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+              "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3), "queries": n1, "ef": ef_op}
     cg.close()
-    return {
-        "metric": "QPS at recall@10>=0.95 (plain bit-exact form)",
+    info = cpu_info()
+    out = {
+        "metric": "QPS at recall@10>=0.95 (reference CPU search, Graph::search)",
         "value": round(qps, 1), "unit": "queries/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)",
+        "data": DATA,
         "config": {"workload": WORKLOAD, "n": N_BASE, "dim": DIM, "k": K, "ef": ef_op,
-                   "step": f"{per_step} queries"},
+                   "step": f"{per_step} queries", "graph": "reference build_graph (graph.h:190-199)",
+                   "graph_build_s": build_s,
+                   "selection": f"smallest ef with recall@10 >= {TARGET_RECALL}+{SELECT_MARGIN} on 500 "
+                                f"calibration queries"},
         "impl": "reference",
         "recall_at_10": round(rec, 4),
-        "ef_curve": curve,
+        "cpu": info,
+        "single_thread": single,
         "cpu_baseline": {"value": round(qps, 1), "unit": "queries/s", "cores": threads,
                          "kind": "reference",
                          "sample": f"{per_step} queries per step, Graph::search (graph.h:33) from "
@@ -681,30 +1010,74 @@ def run_reference(args, ws, rank, local):
         "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    return out, {"ef_curve": curve, "step_s": [round(t, 4) for t in times]}
+
+
+# ------------------------------------------------------------------ output
+
+def compact_line(out: dict, limit: int = LINE_LIMIT) -> str:
+    """The stdout JSON line: `out` as is when it fits `limit` bytes; else the
+    optional per-config summaries are dropped, largest first."""
+    line = json.dumps(out, separators=(",", ":"))
+    if len(line) <= limit:
+        return line
+    out = json.loads(line)
+    for key in ("configs", "reference_gpu_kernel", "roofline_plain", "forms"):
+        sub = out.get(key)
+        if isinstance(sub, dict):
+            for k2 in sorted(sub, key=lambda s: -len(json.dumps(sub[s]))):
+                sub[k2] = "in the details file"
+                line = json.dumps(out, separators=(",", ":"))
+                if len(line) <= limit:
+                    return line
+        out.pop(key, None)
+        line = json.dumps(out, separators=(",", ":"))
+        if len(line) <= limit:
+            return line
+    return line
+
+
+def write_details(path: str, details) -> None:
+    if not path or details is None:
+        return
+    try:
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        with open(path, "w") as f:
+            json.dump(details, f, indent=1, default=str)
+    except OSError as e:
+        log(f"details file not written: {e}")
 
 
 def main(argv=None):
-    global N_BASE, NQ
+    global N_BASE, NQ, NCAL
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--details", default=os.path.join(ROOT, "gpurun_out", "bench_details.json"),
+                    help="side file for curves, sweeps and per-step times ('' = none)")
+    ap.add_argument("--graph", choices=("auto", "gpu", "ref"), default="auto",
+                    help="auto: the reference arm's graph when present, else the GPU builder")
     ap.add_argument("--ref-step-queries", type=int, default=1000)
+    ap.add_argument("--ref-single-queries", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned form")
+    ap.add_argument("--no-queue-sweep", action="store_true")
     ap.add_argument("--train-queries", type=int, default=50_000)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--configs", default="", help="extra workloads, comma separated")
     ap.add_argument("--n", type=int, default=N_BASE, help="base size (profiling cases)")
     ap.add_argument("--nq", type=int, default=NQ, help="queries per GPU (profiling cases)")
     ap.add_argument("--ef", type=int, default=0, help="fixed queue size: skip the sweep")
     ap.add_argument("--bf-words", type=int, default=1024, help="Bloom words with --ef")
     args = ap.parse_args(argv)
     N_BASE, NQ = args.n, args.nq
+    NCAL = min(NCAL, max(NQ, 1000))
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_env()
@@ -712,16 +1085,18 @@ def main(argv=None):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
         backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     try:
         if args.impl == "reference":
-            out = run_reference(args, ws, rank, local)
+            out, details = run_reference(args, ws, rank, local)
         else:
-            out = run_ours(args, ws, rank, local)
+            out, details = run_ours(args, ws, rank, local)
         if rank == 0 and out is not None:
-            print(json.dumps(out), flush=True)
+            write_details(args.details, {"line": out, **(details or {})})
+            print(compact_line(out), flush=True)
     finally:
         if ws > 1:
             import torch.distributed as dist

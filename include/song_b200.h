@@ -105,8 +105,17 @@ typedef struct song_search_opts {
     int bloom_hashes;     /* learned search: Bloom hashes per id (1..4) in place of the
                              index's bf_nhash (BF_NHASH); 0 = the index's value.  Plain
                              searches reject it: they keep the reference's visited set */
-    int reserved[2];
+    int entry;            /* learned search, entry points (SONG_ENTRY_*): 0 = the entry
+                             model's top N_MULTIPROBE hubs; 1 = the N_MULTIPROBE nearest
+                             hubs of the entry stage, no model; 2 = the reference's seeds
+                             p*n/N_MULTIPROBE, no entry stage.  1 and 2 measure what the
+                             entry model and the entry stage contribute              */
+    int reserved;
 } song_search_opts;
+
+#define SONG_ENTRY_MODEL   0
+#define SONG_ENTRY_NEAREST 1
+#define SONG_ENTRY_SEEDS   2
 
 /* Reference defaults of config.h:9-58. */
 void song_params_default(song_params* p);
@@ -192,7 +201,12 @@ song_status song_graph_search_device(song_index* index, const float* d_queries, 
  * counter (a ring of 1024 per index) and its own scratch (entry-stage lists,
  * Graph::search bitmaps) from the index's stream-ordered memory pool, freed
  * on the launching stream.  Host calls on one index are serialised by a
- * lock.
+ * lock.  One thing is shared: the index's error word.  A kernel that meets
+ * an out-of-range id (a corrupted graph or caller seed) sets it instead of
+ * reading out of range, and every host call clears it before its own
+ * launches and reports it after them, so with searches of one index running
+ * on several streams at once an error is reported by whichever host call
+ * reads the word next, not necessarily by the call whose launch set it.
  */
 song_status song_search_device(song_index* index, const void* d_queries, int nq, int k,
                                int ef_search, int32_t* d_ids, song_query_trace* d_traces,
@@ -228,7 +242,10 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
  * Asynchronous on `stream` (a cudaStream_t).  The first call on a device
  * looks up the array's device address, so make that first call before any
  * stream capture.  All calls share the array: calls that overlap on the GPU
- * race with each other.  Produces the same graph as song_build_graph.
+ * race with each other.  The library must not be used on a device after a
+ * cudaDeviceReset (the looked-up address would be stale).  Row words or
+ * floats past dim (ld > dim) are ignored, whatever they hold.  Produces the
+ * same graph as song_build_graph.
  */
 song_status song_build_graph_noalloc(int kind, const void* d_rows, int64_t n, int dim, int ld,
                                      const song_params* params, int batch_ratio,

@@ -20,8 +20,9 @@ variant's constants, and two shared libraries are compiled against them:
   (kernalGraph.h:307-382, hashKernelGraph.h:360-435).  Its kernels only run on
   a GPU host; its builders run anywhere.
 
-The reference sources are read from ``$SONG_REF_DIR`` (default: the mounted
-reference checkout); nothing of them is committed.  Usage::
+The reference sources are read from ``$SONG_REF_DIR``, or else from a
+``reference`` checkout beside this repository (``../reference`` relative to
+the repository root); nothing of them is committed.  Usage::
 
     python oracle/build_ref.py                 # the default variant set
     python oracle/build_ref.py --bs 16 --bfw 16 --pq 256
@@ -37,7 +38,8 @@ import sys
 from dataclasses import dataclass, asdict
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_DIR = os.environ.get("SONG_REF_DIR", "/root/reference")
+REF_DIR = os.environ.get("SONG_REF_DIR") or os.path.normpath(
+    os.path.join(HERE, os.pardir, os.pardir, "reference"))
 OUT_DIR = os.path.join(HERE, "_ref")
 HEADERS = [
     "config.h", "distance.h", "telemetry.h", "graph.h", "kernalGraph.h",
