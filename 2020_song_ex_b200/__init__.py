@@ -115,6 +115,12 @@ class _ServerConfig(C.Structure):
                 ("hbm_budget", C.c_longlong), ("max_ctas", C.c_int), ("idle_exit_us", C.c_int)]
 
 
+class _ServerStats(C.Structure):
+    _fields_ = [("launches", C.c_longlong), ("idle_exits", C.c_longlong),
+                ("poll_cap_exits", C.c_longlong), ("stop_exits", C.c_longlong),
+                ("running", C.c_int)]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -169,6 +175,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_server_run_poisson.argtypes = [vp, vp, ci, vp, vp, vp, C.c_double, C.c_uint, vp, vp,
                                           C.POINTER(C.c_double)]
     L.song_server_destroy.argtypes = [vp]
+    L.song_server_wait.argtypes = [vp, C.c_longlong, C.c_longlong, vp, vp, vp]
+    L.song_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
     L.song_search_device_seeded.argtypes = [vp, C.POINTER(_Opts), vp, ci, ci, ci, vp, ci, vp, vp,
                                             vp, vp]
     L.song_search_device_seeded.restype = C.c_int
@@ -192,7 +200,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.song_exact_knn.argtypes = [vp, i64, ci, vp, ci, ci, vp, vp]
     L.song_exact_knn.restype = C.c_int
     for name in ("song_server_create", "song_server_submit", "song_server_poll",
-                 "song_server_run_poisson", "song_server_destroy"):
+                 "song_server_run_poisson", "song_server_destroy", "song_server_wait",
+                 "song_server_get_stats"):
         getattr(L, name).restype = C.c_int
     for name in ("song_index_create_l2", "song_index_create_hamming", "song_index_destroy",
                  "song_index_info", "song_gpu_search", "song_gpu_search_hamming",
@@ -707,6 +716,22 @@ class Server:
         _check(load_library().song_server_poll(self._h, ticket, ids.ctypes.data, d.ctypes.data,
                                                tr.ctypes.data, C.byref(done)))
         return bool(done.value), ids[:k], d[:k], tr
+
+    def wait(self, ticket: int, k: int, timeout_us: int):
+        """(ids[:k], dists[:k], QueryTrace row) once the ticket finished; raises
+        SongError(SONG_ERR_TIMEOUT) if it has not within timeout_us."""
+        ids = np.empty(self.config.max_k, dtype=np.int32)
+        d = np.empty(self.config.max_k, dtype=np.float32)
+        tr = np.zeros(12, dtype=np.int32)
+        _check(load_library().song_server_wait(self._h, ticket, int(timeout_us), ids.ctypes.data,
+                                               d.ctypes.data, tr.ctypes.data))
+        return ids[:k], d[:k], tr
+
+    def stats(self) -> dict:
+        """Launch count, running flag and why the kernel's warps left (song_server_get_stats)."""
+        st = _ServerStats()
+        _check(load_library().song_server_get_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
 
     def run_poisson(self, queries, ks, efs, flags, rate_qps: float, seed: int = 0):
         """Native Poisson-arrival driver: (latency_ms [nq], ids [nq, max_k], wall_s)."""

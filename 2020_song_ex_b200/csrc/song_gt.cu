@@ -638,7 +638,7 @@ song_status song_exact_knn_device(const float* d_base, int64_t n, int64_t ldb, i
         std::snprintf(buf, sizeof(buf), "exact kNN: %s", cudaGetErrorString(e));
         return song::set_error(SONG_ERR_CUDA, buf);
     }
-    if (err != 0) return song::set_error(SONG_ERR_CUDA, "exact kNN: a bounded wait gave up");
+    if (err != 0) return song::set_error(SONG_ERR_TIMEOUT, "exact kNN: a bounded wait gave up");
     return SONG_OK;
 }
 

@@ -20,6 +20,7 @@
 #include <new>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "song_b200.h"
@@ -32,7 +33,8 @@ struct song_server {
     int dim = 0, num_sms = 0, device = 0, cap_limit = 0, warps = 0;
     int slots = 0, slot_bytes = 0;
     unsigned char* d_ring = nullptr;
-    long long* d_ctrl = nullptr;       // [0] head, [1] tail, [2] stop, [3] last claim time
+    long long* d_ctrl = nullptr;       // [0] head, [1] tail, [2] stop, [3] last claim time,
+                                       // [4..6] warps that left idle / at the poll cap / at stop
     unsigned char* h_stage = nullptr;  // pinned staging of ring slots
     long long* h_tailbuf = nullptr;    // pinned tail values, one per slot
     long long* h_stop = nullptr;       // pinned source of the stop word
@@ -48,6 +50,7 @@ struct song_server {
     cudaEvent_t kdone = nullptr;
     cudaEvent_t pubdone = nullptr;  // the last publish's copies (and entry stage) are done
     bool launched = false;
+    long long launches = 0;
     long long next = 0;  // next ticket
     std::mutex mu;
 };
@@ -85,6 +88,7 @@ song_status ensure_running(song_server* v) {
     if (e != cudaSuccess) return cuda_err(e, "serve launch");
     SRV_CUDA(cudaEventRecord(v->kdone, v->kst), "event");
     v->launched = true;
+    v->launches += 1;
     return SONG_OK;
 }
 
@@ -254,6 +258,7 @@ song_status song_server_create(song_index* index, const song_server_config* cfg,
     s.res_trace = v->h_trace;
     s.res_done = v->h_done;
     s.last_claim = v->d_ctrl + 3;
+    s.exits = v->d_ctrl + 4;
     s.scand = v->d_scand;
     s.sdist = v->d_sdist;
     s.idle_ns = (long long)cfg->idle_exit_us * 1000;
@@ -305,6 +310,38 @@ song_status song_server_poll(song_server* v, long long ticket, int32_t* ids, flo
     std::lock_guard<std::mutex> lock(v->mu);
     if (ticket >= v->next) return song::set_error(SONG_ERR_INVALID_ARG, "ticket not submitted");
     return ensure_running(v);
+}
+
+song_status song_server_wait(song_server* v, long long ticket, long long timeout_us, int32_t* ids,
+                             float* dists, song_query_trace* trace) {
+    using clk = std::chrono::steady_clock;
+    if (!v || ticket < 0 || timeout_us < 0) return song::set_error(SONG_ERR_INVALID_ARG, "bad wait");
+    const auto deadline = clk::now() + std::chrono::microseconds(timeout_us);
+    for (long long spins = 0;; ++spins) {
+        int done = 0;
+        if (song_status st = song_server_poll(v, ticket, ids, dists, trace, &done)) return st;
+        if (done) return SONG_OK;
+        if (clk::now() >= deadline) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "ticket %lld not finished within %lld us", ticket, timeout_us);
+            return song::set_error(SONG_ERR_TIMEOUT, buf);
+        }
+        if (spins > 64) std::this_thread::yield();
+    }
+}
+
+song_status song_server_get_stats(song_server* v, song_server_stats* out) {
+    if (!v || !out) return song::set_error(SONG_ERR_INVALID_ARG, "bad stats call");
+    std::lock_guard<std::mutex> lock(v->mu);
+    long long ex[3] = {0, 0, 0};
+    SRV_CUDA(cudaMemcpyAsync(ex, v->d_ctrl + 4, sizeof ex, cudaMemcpyDeviceToHost, v->cst), "stats copy");
+    SRV_CUDA(cudaStreamSynchronize(v->cst), "stats copy");
+    out->launches = v->launches;
+    out->idle_exits = ex[0];
+    out->poll_cap_exits = ex[1];
+    out->stop_exits = ex[2];
+    out->running = (v->launched && cudaEventQuery(v->kdone) == cudaErrorNotReady) ? 1 : 0;
+    return SONG_OK;
 }
 
 song_status song_server_run_poisson(song_server* v, const float* queries, int nq, const int* ks,

@@ -439,6 +439,24 @@ song_status song_server_submit(song_server* s, const float* queries, int n, cons
 /* *done = 1 and ids/dists/trace (host, nullable) filled when the ticket finished. */
 song_status song_server_poll(song_server* s, long long ticket, int32_t* ids, float* dists,
                              song_query_trace* trace, int* done);
+/* Wait for a ticket at most timeout_us microseconds (host-side, bounded):
+ * SONG_OK with ids/dists/trace filled, or SONG_ERR_TIMEOUT if it has not
+ * finished by then (it may still finish; wait or poll again). */
+song_status song_server_wait(song_server* s, long long ticket, long long timeout_us, int32_t* ids,
+                             float* dists, song_query_trace* trace);
+
+/* The persistent kernel's state: how often it was launched, whether it is
+ * running, and why its warps left -- the server-wide idle time ran out
+ * (idle_exit_us), the cap on empty polls was reached, or the stop word.
+ * Every wait of the kernel is bounded; a later submit relaunches it. */
+typedef struct song_server_stats {
+    long long launches;
+    long long idle_exits;      /* warps that left because nothing was claimed for idle_exit_us */
+    long long poll_cap_exits;  /* warps that left at the cap on consecutive empty polls         */
+    long long stop_exits;      /* warps that left at the stop word                              */
+    int running;               /* 1 while the last launch has not finished                      */
+} song_server_stats;
+song_status song_server_get_stats(song_server* s, song_server_stats* out);
 /* Native Poisson driver: nq requests arriving at rate_qps (exponential gaps,
  * seeded), submitted as they arrive, completions observed by polling.
  * latency_ms[i] = completion - arrival of request i.  ids_out (nullable)

@@ -95,3 +95,38 @@ def test_admission_limits(cuda, song, setup):
     with pytest.raises(song.SongError) as e:  # a budget that holds no slot
         song.Server(g, song.ServerConfig(hbm_budget=64))
     assert e.value.status == song.SONG_ERR_BUDGET
+
+
+def test_idle_wait_runs_out_then_relaunch(cuda, song, setup):
+    """The persistent kernel's idle wait is bounded: with nothing to claim its
+    warps leave after idle_exit_us and the kernel ends cleanly; a later submit
+    relaunches it and the results are the same as searched alone.  A wait on
+    the host with a deadline that passes first reports SONG_ERR_TIMEOUT."""
+    import time
+    m, g, ks, efs, flags = setup
+    cfg = song.ServerConfig(max_k=100, max_ef=256, idle_exit_us=2000)
+    with song.Server(g, cfg) as srv:
+        for rnd in range(2):
+            t0 = srv.submit(m.queries[:32], ks[:32], efs[:32], flags[:32])
+            for i in range(32):
+                ids, _, tr = srv.wait(t0 + i, int(ks[i]), timeout_us=30_000_000)
+                ids_a, tr_a = alone(song, g, m.queries[i], ks[i], efs[i], flags[i], 0.85)
+                np.testing.assert_array_equal(ids, ids_a, err_msg=f"round {rnd} request {i}")
+                np.testing.assert_array_equal(tr, tr_a, err_msg=f"round {rnd} trace {i}")
+            deadline = time.time() + 10
+            st = srv.stats()
+            while st["running"] and time.time() < deadline:  # the idle wait runs out
+                time.sleep(0.01)
+                st = srv.stats()
+            assert st["running"] == 0
+            assert st["launches"] == rnd + 1
+            assert st["idle_exits"] + st["poll_cap_exits"] > 0
+            assert st["stop_exits"] == 0
+        # a deadline of zero: the request was only just published
+        t1 = srv.submit(m.queries[40:41], ks[40:41], efs[40:41], flags[40:41])
+        with pytest.raises(song.SongError) as e:
+            srv.wait(t1, int(ks[40]), timeout_us=0)
+        assert e.value.status == song.SONG_ERR_TIMEOUT
+        ids, _, _ = srv.wait(t1, int(ks[40]), timeout_us=30_000_000)
+        ids_a, _ = alone(song, g, m.queries[40], ks[40], efs[40], flags[40], 0.85)
+        np.testing.assert_array_equal(ids, ids_a)
