@@ -837,9 +837,238 @@ def summary_serving(s):
                         p.get("recall@10")] for p in s["points"]]}
 
 
+C3 = {"n": 1_000_000, "dim": 960, "n_comp": 256, "nq": 1000, "seed": 960}
+C4 = {"n": 1_183_514, "dim": 200, "n_comp": 512, "nq": 10_000, "ntrain": 50_000, "seed": 200}
+C4H = {"n": 290_000, "dim": 256, "n_comp": 256, "nq": 10_000, "bits": 512, "seed": 256}
+C3_EFS = (32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024)
+C4_EFS = (32, 48, 64, 96, 128, 192, 256, 320, 384, 512, 768, 1024)
+HAM_EFS = (32, 50, 64, 128, 256, 512, 1024)
+
+
 def measure_extra_configs(c, details, names):
-    """Other workloads (filled in by later sections)."""
-    return {}
+    """The other workloads, each summarised in one entry of the line's
+    `configs` (the curves go to the side file)."""
+    out = {}
+    for name in names:
+        name = name.strip().lower()
+        t0 = time.time()
+        key = {"c3": "c3_precision", "c4": "c4_angular", "c4h": "c4_hamming"}.get(name, name)
+        try:
+            if name == "c3":
+                out[key] = measure_c3(c, details)
+            elif name == "c4":
+                out[key] = measure_c4(c, details)
+            elif name == "c4h":
+                out[key] = measure_c4h(c, details)
+            elif name:
+                out[key] = {"unavailable": "unknown config"}
+        except Exception as e:  # one workload failing must not lose the line
+            out[key] = {"error": f"{type(e).__name__}: {e}"[:200]}
+        log(f"[configs] {name} {time.time() - t0:.1f} s: {out.get(key)}")
+        c.torch.cuda.empty_cache()
+    return out
+
+
+def _sweep(c, efs, run, gt, k, nq):
+    """Points (ef, recall, qps) of `run(ef)` (which searches the calibration
+    queries and returns (ids, ms)) until recall@k reaches the target plus the
+    margin."""
+    pts = []
+    for ef in efs:
+        ids, ms = run(ef)
+        rec = float(c.ds.recall_at_k(ids, gt, k).mean())
+        pts.append({"ef": ef, "recall": round(rec, 4), "qps": round(nq / ms * 1e3)})
+        if rec >= TARGET_RECALL + SELECT_MARGIN:
+            break
+    return pts
+
+
+def _op(pts):
+    ok = [p for p in pts if p["recall"] >= TARGET_RECALL + SELECT_MARGIN]
+    return (max(ok, key=lambda p: p["qps"]), True) if ok else (max(pts, key=lambda p: p["recall"]), False)
+
+
+def measure_c3(c, details):
+    """C3, precision form: 1M x 960 non-negative mixture, L1-normalised; BF16
+    and per-vector-scaled FP8 rows with FP32 accumulation and an exact FP32
+    re-rank of the final results queue, against the plain FP32 form on the
+    same graph.  Operating points on 1,000 calibration queries, reported on
+    1,000 others; distance error of the returned results against FP64."""
+    torch, song, ds = c.torch, c.song, c.ds
+    n, dim, nq = c.args.c3_n or C3["n"], C3["dim"], C3["nq"]
+    t0 = time.time()
+    m = ds.l1_mixture(n, 2 * nq, dim=dim, n_comp=C3["n_comp"], seed=C3["seed"])
+    gen_s = time.time() - t0
+    t0 = time.time()
+    adj = song.build_graph(m.base, song.Params(block_size=32, fixed_degree=31), batch_ratio=32)
+    build_s = time.time() - t0
+    cal, ev = m.queries[:nq], m.queries[nq:]
+    gt_ev, _ = c.gtm.knn(m.base, ev, K)
+    gt_cal, _ = c.gtm.knn(m.base, cal, K)
+    g = song.KernelGraph(n, dim, m.base, song.Params(pq_size=1024, bf_words=512), adj=adj)
+    g.upload_to_gpu()
+    dcal, dev_q = torch.from_numpy(cal).to(c.dev), torch.from_numpy(ev).to(c.dev)
+    ids_d = torch.empty((nq, K), dtype=torch.int32, device=c.dev)
+    dist_d = torch.empty((nq, K), dtype=torch.float32, device=c.dev)
+    tr_d = torch.empty((nq, 12), dtype=torch.int32, device=c.dev)
+    st = c.stream
+    base_t = torch.from_numpy(m.base).to(c.dev)
+    res, curves = {}, {}
+    for form, prec, rerank in (("fp32_plain", song.PREC_FP32, False), ("bf16_rerank", song.PREC_BF16, True),
+                               ("fp8_rerank", song.PREC_FP8, True), ("fp8_no_rerank", song.PREC_FP8, False)):
+        if prec != song.PREC_FP32:
+            song.set_precision(g, prec)
+        opts = song.SearchOpts(precision=prec, rerank=rerank)
+
+        def run(ef, q=dcal):
+            ms = launch_ms(torch, st, lambda: song.search_device_ex(g, opts, q, nq, K, ef, ids_d, dist_d,
+                                                                     None, stream=st))
+            return ids_d.cpu().numpy(), ms
+
+        pts = _sweep(c, C3_EFS, run, gt_cal, K, nq)
+        op, ok = _op(pts)
+        song.search_device_ex(g, opts, dev_q, nq, K, op["ef"], ids_d, dist_d, tr_d, stream=st)
+        st.synchronize()
+        ids = ids_d.cpu().numpy()
+        tr = tr_d.cpu().numpy()
+        d32 = dist_d.clone()
+        ms = launch_ms(torch, st, lambda: song.search_device_ex(g, opts, dev_q, nq, K, op["ef"], ids_d,
+                                                                 dist_d, None, stream=st), reps=5)
+        rec = float(ds.recall_at_k(ids, gt_ev, K).mean())
+        # distance error of every returned result against FP64
+        valid = torch.from_numpy(ids >= 0).to(c.dev)
+        sel = torch.from_numpy(np.maximum(ids, 0).astype(np.int64)).to(c.dev)
+        d64 = ((base_t[sel].double() - dev_q[:, None, :].double()) ** 2).sum(-1)
+        rel = ((d32.double() - d64).abs() / d64.clamp_min(1e-300))[valid]
+        E, X = tr[:, 5].astype(np.float64), tr[:, 2].astype(np.float64)
+        s_bytes = {song.PREC_FP32: dim * 4, song.PREC_BF16: dim * 2, song.PREC_FP8: dim + 4}[prec]
+        b = E * s_bytes + X * BLOCK_SIZE * 4 + dim * 4 + K * 4
+        if rerank:
+            b = b + np.minimum(op["ef"], 1024) * dim * 4
+        res[form] = {"ef": op["ef"], "reached_on_calibration": ok, "recall_at_10": round(rec, 4),
+                     "qps": round(nq / ms * 1e3), "kernel_ms": round(ms, 4),
+                     "dist_rel_err_max": float(f"{rel.max().item():.3e}"),
+                     "dist_rel_err_mean": float(f"{rel.mean().item():.3e}"),
+                     "gather_gbs": round(float(b.sum()) / (ms / 1e3) / 1e9, 1),
+                     "mean_expanded": round(float(X.mean()), 1)}
+        curves[form] = pts
+    g.close()
+    del base_t
+    details["c3"] = {"forms": res, "curves": curves,
+                     "timing_s": {"generate": round(gen_s, 1), "gpu_build": round(build_s, 1)}}
+    best = max((v for k2, v in res.items() if k2.endswith("_rerank")), key=lambda v: v["qps"])
+    return {"workload": f"{n} x {dim} L1-normalised 256-comp mixture, {nq} eval queries, deg 31, k=10",
+            "cols": "ef, recall@10, qps, dist rel err max vs fp64",
+            **{k2: [v["ef"], v["recall_at_10"], v["qps"], v["dist_rel_err_max"]] for k2, v in res.items()},
+            "lowp_rerank_over_fp32": round(best["qps"] / max(res["fp32_plain"]["qps"], 1), 2),
+            "build_s": round(build_s, 1)}
+
+
+def measure_c4(c, details):
+    """C4, learned form on angular data: 1,183,514 x 200 L2-normalised
+    anisotropic mixture; models trained on 50,000 held-out queries; plain and
+    learned forms at recall@k >= 0.95 (chosen on calibration queries) for
+    k = 10 and 100 (k = 100: the learned entry without the stop model)."""
+    torch, song, ds, gtm = c.torch, c.song, c.ds, c.gtm
+    n, dim, nq, ntr = c.args.c4_n or C4["n"], C4["dim"], C4["nq"], C4["ntrain"]
+    t0 = time.time()
+    m = ds.angular_mixture(n, 2 * nq + ntr, dim=dim, n_comp=C4["n_comp"], seed=C4["seed"])
+    ev, cal, train = m.queries[:nq], m.queries[nq:2 * nq], m.queries[2 * nq:]
+    gen_s = time.time() - t0
+    t0 = time.time()
+    adj = song.build_graph(m.base, song.Params(block_size=32, fixed_degree=31), batch_ratio=32)
+    build_s = time.time() - t0
+    gt100, _ = gtm.knn(m.base, ev, 100)
+    gt_cal, _ = gtm.knn(m.base, cal, 100)
+    nn1, _ = gtm.knn(m.base, train, 1)
+    g = song.KernelGraph(n, dim, m.base, song.Params(pq_size=1024, bf_words=512), adj=adj)
+    g.upload_to_gpu()
+    dev_q, dcal = torch.from_numpy(ev).to(c.dev), torch.from_numpy(cal).to(c.dev)
+    st = c.stream
+    out, curves = {}, {}
+    for k in (10, 100):
+        ids_d = torch.empty((nq, k), dtype=torch.int32, device=c.dev)
+
+        def plain(ef, q=dcal):
+            ms = launch_ms(torch, st, lambda: song.search_device(g, q, nq, k, ef, ids_d, None, stream=st))
+            return ids_d.cpu().numpy(), ms
+
+        pts = _sweep(c, [e for e in C4_EFS if e >= k], plain, gt_cal[:, :k], k, nq)
+        op, ok = _op(pts)
+        ids, ms = plain(op["ef"], dev_q)
+        out[f"plain_k{k}"] = {"ef": op["ef"], "qps": round(nq / ms * 1e3), "reached": ok,
+                              "recall": round(float(ds.recall_at_k(ids, gt100[:, :k], k).mean()), 4)}
+        curves[f"plain_k{k}"] = pts
+    t1 = time.time()
+    song.learn(g, torch.from_numpy(train).to(c.dev), ntr,
+               torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(c.dev),
+               song.LearnParams(k=K, ef=128))
+    learn_s = time.time() - t1
+    for k, thr in ((10, 0.9), (10, 1.0), (100, 1.0)):
+        ids_d = torch.empty((nq, k), dtype=torch.int32, device=c.dev)
+        best = None
+        for beam in (1, 2, 4):
+            opts = song.SearchOpts(learned=True, stop_threshold=thr, beam=beam, bloom_hashes=2)
+
+            def learned(ef, q=dcal):
+                ms = launch_ms(torch, st, lambda: song.search_device_ex(g, opts, q, nq, k, ef, ids_d, None,
+                                                                         None, stream=st))
+                return ids_d.cpu().numpy(), ms
+
+            pts = _sweep(c, [e for e in C4_EFS if e >= k], learned, gt_cal[:, :k], k, nq)
+            op, ok = _op(pts)
+            curves[f"learned_k{k}_thr{thr}_beam{beam}"] = pts
+            if ok and (best is None or op["qps"] > best[0]["qps"]):
+                best = (op, beam, opts)
+        if best is None:
+            out[f"learned_k{k}_thr{thr}"] = {"reached": False}
+            continue
+        op, beam, opts = best
+        ms = launch_ms(torch, st, lambda: song.search_device_ex(g, opts, dev_q, nq, k, op["ef"], ids_d, None,
+                                                                 None, stream=st), reps=5)
+        ids = ids_d.cpu().numpy()
+        out[f"learned_k{k}_thr{thr}"] = {"ef": op["ef"], "beam": beam, "qps": round(nq / ms * 1e3),
+                                         "recall": round(float(ds.recall_at_k(ids, gt100[:, :k], k).mean()), 4)}
+    g.close()
+    details["c4"] = {"points": out, "curves": curves,
+                     "timing_s": {"generate": round(gen_s, 1), "gpu_build": round(build_s, 1),
+                                  "learn": round(learn_s, 1)}}
+    return {"workload": f"{n} x {dim} L2-normalised 512-comp anisotropic mixture, {nq} eval queries, deg 31",
+            "cols": "ef, qps, recall@k",
+            **{k2: [v.get("ef"), v.get("qps"), v.get("recall")] for k2, v in out.items()},
+            "build_s": round(build_s, 1)}
+
+
+def measure_c4h(c, details):
+    """C4, Hamming variant: 512-bit sign-random-projection codes (BitHash,
+    bitHash.h:17-56, seed 42) of a 290,000 x 256 L2-normalised base; NSW graph
+    on the codes (hashKernelGraph.h:196-207); recall@10 against the exact L2
+    neighbours of the vectors, as the reference measures it."""
+    torch, song, ds, gtm = c.torch, c.song, c.ds, c.gtm
+    n, dim, nq, bits = C4H["n"], C4H["dim"], C4H["nq"], C4H["bits"]
+    m = ds.angular_mixture(n, nq, dim=dim, n_comp=C4H["n_comp"], seed=C4H["seed"])
+    bh = song.BitHash(dim, seed=42, hash_bits=bits)
+    codes, qcodes = bh.project_all(m.base), bh.project_all(m.queries)
+    t0 = time.time()
+    adj = song.build_graph(codes, song.Params(block_size=32, fixed_degree=31), kind=song.KIND_HAMMING,
+                           batch_ratio=32)
+    build_s = time.time() - t0
+    gt, _ = gtm.knn(m.base, m.queries, K)
+    g = song.HashKernelGraph(n, codes, song.Params(pq_size=1024, bf_words=512), adj=adj)
+    g.upload_to_gpu()
+    dq = torch.from_numpy(np.ascontiguousarray(qcodes).view(np.int32)).to(c.dev)
+    ids_d = torch.empty((nq, K), dtype=torch.int32, device=c.dev)
+    pts = []
+    for ef in HAM_EFS:
+        ms = launch_ms(torch, c.stream, lambda: song.search_device(g, dq, nq, K, ef, ids_d, None,
+                                                                   stream=c.stream), reps=3)
+        rec = float(ds.recall_at_k(ids_d.cpu().numpy(), gt, K).mean())
+        pts.append({"ef": ef, "recall": round(rec, 4), "qps": round(nq / ms * 1e3)})
+    g.close()
+    details["c4_hamming"] = {"curve": pts, "gpu_build_s": round(build_s, 1)}
+    return {"workload": f"{n} x {dim} -> {bits}-bit codes, {nq} queries, deg 31, k=10",
+            "cols": "ef: qps, recall@10 (vs exact L2 of the vectors)",
+            **{f"ef{p['ef']}": [p["qps"], p["recall"]] for p in pts}, "build_s": round(build_s, 1)}
 
 
 def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
@@ -1070,7 +1299,9 @@ def main(argv=None):
     ap.add_argument("--train-queries", type=int, default=50_000)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
-    ap.add_argument("--configs", default="", help="extra workloads, comma separated")
+    ap.add_argument("--configs", default="", help="extra workloads, comma separated (c3, c4, c4h)")
+    ap.add_argument("--c3-n", type=int, default=0, help="C3 base size (0 = 1,000,000)")
+    ap.add_argument("--c4-n", type=int, default=0, help="C4 base size (0 = 1,183,514)")
     ap.add_argument("--n", type=int, default=N_BASE, help="base size (profiling cases)")
     ap.add_argument("--nq", type=int, default=NQ, help="queries per GPU (profiling cases)")
     ap.add_argument("--ef", type=int, default=0, help="fixed queue size: skip the sweep")
