@@ -43,9 +43,6 @@ struct song_index {
     int num_sms = 0;
     void* d_base = nullptr;
     int32_t* d_adj = nullptr;
-    // Bloom positions of every adjacency slot's id (bf_words <= 1024): the
-    // search loads them with the row instead of hashing each neighbour
-    uint64_t* d_bpos = nullptr;
     unsigned* d_counter = nullptr;  // ring of work counters, one per launch (kCounterRing)
     unsigned counter_next = 0;
     int* d_err = nullptr;
@@ -153,7 +150,6 @@ void free_index(song_index* x) {
     cudaSetDevice(x->device);
     cudaFree(x->d_base);
     cudaFree(x->d_adj);
-    cudaFree(x->d_bpos);
     cudaFree(x->d_counter);
     cudaFree(x->d_err);
     cudaFree(x->d_q);
@@ -232,16 +228,6 @@ song_status create_common(int kind, const void* rows, int64_t n, int dim, const 
     // a pageable cudaMemcpy may return before its DMA lands: finish the legacy
     // stream before x->stream (non-blocking) reads the uploaded rows and adjacency
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
-    if (e == cudaSuccess && song::bloom_table_supported(params->bf_words)) {
-        const int64_t slots = n * (int64_t)params->block_size;
-        if (cudaMalloc(&x->d_bpos, (size_t)slots * sizeof(uint64_t)) == cudaSuccess) {
-            e = song::build_bloom_table(x->d_adj, slots, params->bf_words, x->d_bpos, x->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
-        } else {
-            (void)cudaGetLastError();  // an acceleration only: search without it
-            x->d_bpos = nullptr;
-        }
-    }
     if (e == cudaSuccess && kind == SONG_KIND_L2 && x->range.int_base && x->range.lo >= 0.0f &&
         x->range.hi <= 255.0f && dim <= song::kU8MaxDim) {
         x->u8_ld = song::u8_row_bytes(dim);
@@ -361,7 +347,6 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
     std::memset(a, 0, sizeof *a);
     a->base = x->d_base;
     a->adj = x->d_adj;
-    a->bpos = x->d_bpos;
     a->queries = d_q;
     a->out = d_ids;
     a->trace = d_tr;

@@ -39,7 +39,6 @@ struct SearchArgs {
     int tm_warp_cols;        // TMEM columns of one warp's queue ids (set by launch_search)
     int int_base;            // 1: every base value is an integer in [base_min, base_max]
     float base_min, base_max;
-    const uint64_t* bpos;    // [n x block_size] Bloom positions of each adjacency slot's id, or nullptr
     const uint8_t* u8;       // base values as bytes [n x u8_ld] when all are integers in [0, 255]
     int u8_ld;               // bytes per byte row (multiple of 16)
     // precision form (prec != SONG_PREC_FP32)
@@ -138,13 +137,6 @@ constexpr int kU8MaxDim = 256;
 int u8_row_bytes(int dim);
 cudaError_t convert_rows_u8(const float* d_rows, int64_t n, int dim, int ld, uint8_t* d_out,
                             int out_ld, cudaStream_t st);
-
-// Bloom positions of every adjacency slot (filters of at most 2^16 bits,
-// i.e. bf_words <= 1024): d_out[i] packs bf_pos(h, adj[i]) for h = 0..3 in
-// 16-bit fields.  Stream-ordered.
-bool bloom_table_supported(int bf_words);
-cudaError_t build_bloom_table(const int32_t* d_adj, int64_t slots, int bf_words, uint64_t* d_out,
-                              cudaStream_t st);
 
 // Row stride (elements) the kernels use for `dim` elements of `kind`.
 int search_row_stride(int kind, int dim);

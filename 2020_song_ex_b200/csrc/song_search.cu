@@ -118,6 +118,12 @@ struct Queue {
     int cap;
     unsigned xb[GPL], xi[GPL];  // group maximum bits, first slot holding it (NONE = empty)
     unsigned nb[GPL], ni[GPL];  // group minimum bits, first slot holding it
+    // The queue's maximum and its first slot while cx holds (results queue
+    // only: its maximum is read at every early-stop check and push): kept
+    // through appends and evictions instead of recomputed from the group
+    // summaries each time.
+    unsigned cxb, cxi;
+    bool cx;
 };
 
 // Id of slot s (warp-uniform s; every lane gets it).
@@ -151,6 +157,7 @@ __device__ __forceinline__ void q_init(Queue<GPL, TM>& q, float* d, int* id, uin
     q.tid = tid;
     q.sz = 0;
     q.cap = cap;
+    q.cx = false;
 #pragma unroll
     for (int r = 0; r < GPL; ++r) {
         q.xb[r] = 0u;
@@ -233,8 +240,20 @@ __device__ __forceinline__ void q_remove(Queue<GPL, TM>& q, int hole, int lane) 
     }
     __syncwarp();
     q.sz = last;
+    q.cx = false;
     group_update<MIN>(q, hole >> 5, lane);
     if ((last >> 5) != (hole >> 5)) group_update<MIN>(q, last >> 5, lane);
+}
+
+// Maximum and its first slot (gpuHeap.h:29, :73), from the cache when it holds.
+template <int GPL, int TM>
+__device__ __forceinline__ void root_max_c(Queue<GPL, TM>& q, unsigned& mb, unsigned& mi) {
+    if (!q.cx) {
+        root_max(q, q.cxb, q.cxi);
+        q.cx = true;
+    }
+    mb = q.cxb;
+    mi = q.cxi;
 }
 
 // Id of slot `hole`, then q_remove(hole): the same queue afterwards, with the
@@ -266,6 +285,7 @@ __device__ __forceinline__ int q_pop(Queue<GPL, TM>& q, int hole, int lane) {
         }
         __syncwarp();
         q.sz = last;
+        q.cx = false;
         group_update<MIN>(q, hole >> 5, lane);
         if ((last >> 5) != (hole >> 5)) group_update<MIN>(q, last >> 5, lane);
         return id;
@@ -276,7 +296,8 @@ __device__ __forceinline__ int q_pop(Queue<GPL, TM>& q, int hole, int lane) {
 // Candidates::push / Results::try_push (gpuHeap.h:23-36, :68-77).
 // Returns how many pushes were accepted.  `stage` (32 ints, TM = 1 only)
 // receives the ids in rank order for the column writes of an append.
-template <bool MIN, int GPL, int TM>
+// RC: keep the queue's cached maximum (cxb, cxi) current.
+template <bool MIN, bool RC = false, int GPL, int TM>
 __device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, int nb, int lane,
                                       int* stage) {
     if (N == 0u) return 0;
@@ -304,13 +325,23 @@ __device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, in
             }
             __syncwarp();
         }
+        if (RC && q.cx) {  // the appended entries sit after every slot: only a larger one moves the maximum
+            const bool app = mine && rank < a;
+            const unsigned am = __reduce_max_sync(FULL, app ? fbits(d) : 0u);
+            if (am > q.cxb) {
+                const int fl = __ffs(__ballot_sync(FULL, app && fbits(d) == am)) - 1;
+                q.cxb = am;
+                q.cxi = (unsigned)(q.sz + __popc(N & lanemask_lt(fl)));
+            }
+        }
         q.sz += a;
         for (int g = g0; g <= g1; ++g) group_update<MIN>(q, g, lane);
         acc = a;
     }
     if (nm > room) {
         unsigned M, fi;
-        root_max(q, M, fi);
+        if constexpr (RC) root_max_c(q, M, fi);
+        else root_max(q, M, fi);
         unsigned rest = __ballot_sync(FULL, mine && rank >= room && fbits(d) < M);
         while (rest) {
             const int j = __ffs(rest) - 1;
@@ -324,6 +355,11 @@ __device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, in
             root_max(q, M, fi);
             rest &= ~(1u << j);
             rest &= __ballot_sync(FULL, fbits(d) < M);
+        }
+        if constexpr (RC) {
+            q.cxb = M;
+            q.cxi = fi;
+            q.cx = true;
         }
     }
     return acc;
@@ -347,24 +383,6 @@ __device__ __forceinline__ uint32_t bf_pos(int h, uint32_t x, const BloomCfg& bc
     return bc.shift >= 0 ? (uint32_t)(y & (bc.nbits - 1)) : (uint32_t)(y % bc.nbits);
 }
 
-// Bloom positions of every adjacency slot's id, for filters of at most 2^16
-// bits: slot i holds bf_pos(h, adj[i]) in bits 16h..16h+15 for h = 0..3
-// (0 for an empty slot).  The search then loads a row's positions beside
-// the row instead of hashing each id: the hash is a pure function of the
-// id, so the positions -- and every result -- are the same.
-__global__ void bloom_table_kernel(const int32_t* __restrict__ adj, int64_t slots, BloomCfg bc,
-                                   uint64_t* __restrict__ out) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= slots) return;
-    const int32_t v = adj[i];
-    uint64_t w = 0;
-    if (v >= 0) {
-#pragma unroll
-        for (int h = 0; h < 4; ++h) w |= (uint64_t)bf_pos(h, (uint32_t)v, bc) << (16 * h);
-    }
-    out[i] = w;
-}
-
 // Bloom test-and-set of one chunk of up to 32 ids (lane j = j-th id of the
 // row, nb < 0 = empty slot), equivalent to the reference's
 //   for j: if (!bf_test(nb_j)) { bf_set(nb_j); new_j = true; }
@@ -380,11 +398,8 @@ __global__ void bloom_table_kernel(const int32_t* __restrict__ adj, int64_t slot
 // (rare with a large filter) every lane checks its missing positions against
 // those of the lanes before it.  The final filter is B0 plus all positions of
 // the new ids either way, as in the reference.
-//
-// With `tab`, `pw` holds the id's positions precomputed (16 bits per hash,
-// hash h in bits 16h..16h+15; see bloom_table_kernel) instead of hashing here.
 __device__ __forceinline__ unsigned bloom_chunk(uint64_t* bloom, int nb, const BloomCfg& bc,
-                                                int lane, bool tab = false, uint64_t pw = 0) {
+                                                int lane) {
     uint32_t pos[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
     uint32_t wd[4] = {0, 0, 0, 0}, bt[4] = {0, 0, 0, 0};
     unsigned unc = 0;
@@ -392,8 +407,7 @@ __device__ __forceinline__ unsigned bloom_chunk(uint64_t* bloom, int nb, const B
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
             if (h < bc.nhash) {
-                const uint32_t p = tab ? (uint32_t)(pw >> (16 * h)) & 0xffffu
-                                       : bf_pos(h, (uint32_t)nb, bc);
+                const uint32_t p = bf_pos(h, (uint32_t)nb, bc);
                 pos[h] = p;
                 wd[h] = bc.shift >= 0 ? (p & bc.wmask) : (p % bc.words);
                 bt[h] = bc.shift >= 0 ? (p >> bc.shift) : (p / bc.words);
@@ -1272,9 +1286,6 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         // first chunk of each adjacency row; learned searches with beam > 1 expand up
         // to 3 more rows this step (BLOCK_SIZE <= 32: one chunk per row)
         int first = -1, first2 = -1, first3 = -1, first4 = -1;
-        // the rows' precomputed Bloom positions (a.bpos), loaded beside the rows
-        uint64_t pfirst = 0;
-        const uint64_t* prow = nullptr;
         int nrows = 1;
         if (seeding) {
             limit = n_seeds;  // seeds p*n/N_MULTIPROBE (kernalGraph.h:214-231)
@@ -1287,14 +1298,11 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             limit = a.block_size;
             arow = a.adj + (int64_t)cn * a.block_size;
             if (lane < limit) first = __ldg(arow + lane);
-            if (LM == 0 && a.bpos != nullptr) {  // learned instances hash (their registers are spoken for)
-                prow = a.bpos + (int64_t)cn * a.block_size;
-                if (lane < limit) pfirst = __ldg(prow + lane);
-            }
             tr.expanded_nodes += 1;
             unsigned wb = 0xffffffffu, wi;
             if (res.sz == res.cap) {  // early stop: full and strictly worse than the worst
-                root_max(res, wb, wi);
+                if constexpr (LM == 0) root_max_c(res, wb, wi);  // cached: plain searches only
+                else root_max(res, wb, wi);
                 if (fbits(cmin) > wb) {
                     tr.early_stopped = 1;
                     break;
@@ -1383,7 +1391,6 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
         for (int c0 = 0; c0 < limit; c0 += 32) {
             const int j = c0 + lane;
             int nb = -1;
-            uint64_t pw = 0;
             if (j < limit) {
                 if (seeding) {
                     nb = (given_seeds || (LM > 0 && seed_id >= 0)) ? seed_id
@@ -1391,8 +1398,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                                                           (unsigned long long)a.n_multiprobe);
                 } else if (rr == 0) {
                     nb = c0 == 0 ? first : __ldg(arow + j);
-                    if (prow != nullptr) pw = c0 == 0 ? pfirst : __ldg(prow + j);
-                } else {  // beam rows: one chunk each (their Bloom positions are hashed here)
+                } else {  // beam rows: one chunk each
                     nb = rr == 1 ? first2 : (rr == 2 ? first3 : first4);
                 }
             }
@@ -1400,7 +1406,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 atomicExch(a.err, 1);
                 nb = -1;
             }
-            const unsigned N = bloom_chunk(bloom, nb, bc, lane, rr == 0 && prow != nullptr, pw);
+            const unsigned N = bloom_chunk(bloom, nb, bc, lane);
             const float d = distances(nb, N);
             const int c = __popc(N);
             if (seeding) {
@@ -1412,7 +1418,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             tr.visited_nodes += c;
             tr.distance_evals += c;
             const int pf = q_push<true>(cand, N, d, nb, lane, rows);
-            const int pr = q_push<false>(res, N, d, nb, lane, rows);
+            const int pr = q_push<false, LM == 0>(res, N, d, nb, lane, rows);
             tr.frontier_pushes += pf;
             tr.result_updates += pr;
             if constexpr (LM == 1 || LM == 2) {
@@ -1681,22 +1687,6 @@ void tm_layout(int query_floats, bool cand_in_tmem, SearchArgs* a) {
 }  // namespace
 
 int u8_row_bytes(int dim) { return round_up(dim, 16); }
-
-bool bloom_table_supported(int bf_words) { return bf_words >= 1 && (int64_t)bf_words * 64 <= 65536; }
-
-cudaError_t build_bloom_table(const int32_t* d_adj, int64_t slots, int bf_words, uint64_t* d_out,
-                              cudaStream_t st) {
-    if (!bloom_table_supported(bf_words)) return cudaErrorInvalidValue;
-    if (slots <= 0) return cudaSuccess;
-    BloomCfg bc;
-    bc.words = (uint32_t)bf_words;
-    bc.nbits = (uint64_t)bf_words * 64ull;
-    bc.shift = (bf_words & (bf_words - 1)) == 0 ? __builtin_ctz((unsigned)bf_words) : -1;
-    bc.wmask = (uint32_t)bf_words - 1u;
-    bc.nhash = 4;
-    bloom_table_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, st>>>(d_adj, slots, bc, d_out);
-    return cudaGetLastError();
-}
 
 cudaError_t convert_rows_u8(const float* d_rows, int64_t n, int dim, int ld, uint8_t* d_out,
                             int out_ld, cudaStream_t st) {
