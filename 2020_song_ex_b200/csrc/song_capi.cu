@@ -113,7 +113,9 @@ song_status cuda_fail(cudaError_t e, const char* what) {
 
 // Each launch takes the next work counter of a ring, so launches that
 // overlap on different streams do not share one; a counter is reused after
-// kCounterRing launches on the same index.
+// kCounterRing launches on the same index.  A ring slot is a pair (work
+// counter, CTAs done): search launches leave it at zero when they finish,
+// so none needs a memset before it (the ring is zeroed once, at creation).
 constexpr unsigned kCounterRing = 1024;
 
 song_status check_params(const song_params* p) {
@@ -201,7 +203,8 @@ song_status create_common(int kind, const void* rows, int64_t n, int dim, const 
     const size_t row_bytes = (size_t)x->ld * 4;
     if (e == cudaSuccess) e = cudaMalloc(&x->d_base, (size_t)n * row_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&x->d_adj, (size_t)n * params->block_size * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&x->d_counter, kCounterRing * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&x->d_counter, 2 * kCounterRing * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(x->d_counter, 0, 2 * kCounterRing * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&x->d_err, 256);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
@@ -450,9 +453,9 @@ song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
         a.ecand = ecand;
         a.edist = edist;
     }
-    unsigned* ctr = x->d_counter + (x->counter_next++ % kCounterRing);
+    unsigned* ctr = x->d_counter + 2 * (x->counter_next++ % kCounterRing);
     a.counter = ctr;
-    SONG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), st), "counter reset");
+    a.done = ctr + 1;
     cudaError_t e = song::launch_search(x->kind, a, x->num_sms, st);
     if (e != cudaSuccess) return cuda_fail(e, "search launch");
     return SONG_OK;
@@ -804,13 +807,16 @@ song_status graph_search_launch(song_index* x, const float* d_q, int nq, int k, 
     CallScratch cs(x, st);
     uint32_t* visited = nullptr;
     SONG_CUDA(cs.get(&visited, (size_t)warps * vwords * 4), "visited bitmaps");
-    unsigned* ctr = x->d_counter + (x->counter_next++ % kCounterRing);
+    unsigned* ctr = x->d_counter + 2 * (x->counter_next++ % kCounterRing);
     SONG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), st), "counter reset");
     cudaError_t e = song::launch_graph_search((const float*)x->d_base, x->ld, x->dim, x->d_adj,
                                               x->p.block_size, x->n, d_q, nq, k, ef,
                                               x->p.n_multiprobe, d_ids, d_tr, ctr, x->d_err,
                                               visited, warps, x->num_sms, st);
     if (e != cudaSuccess) return cuda_fail(e, "Graph::search launch");
+    // this kernel does not return its counter to zero itself: the ring slot
+    // must be zero for the search launch that takes it next
+    SONG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), st), "counter reset");
     return SONG_OK;
 }
 
@@ -934,7 +940,9 @@ song_status song_index_learn(song_index* x, const song_learn_params* lp,
         cudaFree(d_ids);
         return s;
     }
-    a.counter = x->d_counter;
+    unsigned* ctr = x->d_counter + 2 * (x->counter_next++ % kCounterRing);
+    a.counter = ctr;
+    a.done = ctr + 1;
     a.ckpt_every = lp->ckpt_every;
     a.min_expansions = lp->min_expansions;
     // The entry stage: a hub set of entry_hubs nodes (a seeded sample) laid out

@@ -19,6 +19,7 @@ struct SearchArgs {
     int32_t* out;            // [nq x k], best-first, -1 padded
     song_query_trace* trace; // [nq] or nullptr
     unsigned* counter;       // work counter: must be 0 at launch
+    unsigned* done;          // nullable: CTAs past their loop; the last one zeroes counter and done
     int* err;                // set non-zero if an adjacency entry is out of range
     int64_t n;
     int dim;                 // elements compared per row (floats or u32 words)

@@ -1447,6 +1447,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
             a.tr_final_kth[qid] = ss.kth;
         }
     }
+    // a launch that may have started before the previous one on its stream
+    // finished writes nothing until that launch is complete
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     float* outd = a.out_dist ? a.out_dist + (int64_t)qid * a.k : nullptr;
     if (DT != SONG_PREC_FP32 && a.rerank)
         tr.result_count = rerank_finish(a, res, cand, sq, a.out + (int64_t)qid * a.k, outd, lane);
@@ -1518,6 +1521,11 @@ __global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads)
         if (qid >= a.nq) break;
         search_query<KIND, NE, GPL, DT, LM, TM, TMC>(a, qid, ws, lane, tbase);
     }
+    // Every query of this launch has been claimed: a search launched after
+    // this one on the stream with programmatic serialization may start on
+    // the resources this launch's tail leaves idle (it reads only the index
+    // and its own queries, and waits for this launch before it writes).
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if constexpr (TM) {  // every warp is done with TMEM before it is freed
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
@@ -1525,6 +1533,19 @@ __global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads)
         if (warp == 0)
             asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                          :: "r"(tm_slot), "r"(a.tm_cols) : "memory");
+    }
+    if (a.done != nullptr) {
+        // The last CTA past its loop returns the work counter to zero for the
+        // launch that takes this ring slot next, so no memset has to sit
+        // between two launches on the stream.
+        if constexpr (!TM) __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(a.done, 1u) == gridDim.x - 1) {
+                atomicExch(a.counter, 0u);
+                atomicExch(a.done, 0u);
+            }
+        }
     }
 }
 
@@ -1846,7 +1867,22 @@ cudaError_t launch_search(int kind, const SearchArgs& args, int num_sms, cudaStr
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int64_t need = ((int64_t)a.nq + warps - 1) / warps;
     const int grid = (int)std::min<int64_t>((int64_t)per_sm * num_sms, need);
-    fn<<<grid, warps * 32, smem, stream>>>(a);
+    // Plain searches (no learned stage, no caller seeds: nothing they read
+    // can come from the launch before them) with a self-resetting counter
+    // may overlap the previous search launch's tail on the same stream.
+    const bool overlap = a.done != nullptr && a.lm == 0 && a.qseeds == nullptr;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)(warps * 32));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = overlap ? 1 : 0;
+    e = cudaLaunchKernelEx(&cfg, fn, a);
+    if (e != cudaSuccess) return e;
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return cudaGetLastError();
 }
