@@ -1080,11 +1080,17 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     bc.nhash = a.bf_nhash;
 
     // Query in registers (and shared memory for the generic L2 path).
+    // NE < 0 (byte-row instances, an index with byte rows, dim <= 32 * 4 * -NE):
+    // only the query's bytes stay in registers; a query that is not integral
+    // in [0, 255] takes the generic exact path reading its floats from global
+    // memory.  Fewer live registers let more queries reside per SM.
+    constexpr bool kU8 = KIND == 0 && NE < 0;
     constexpr bool kIntPath = KIND == 0 && NE > 0 && DT == SONG_PREC_FP32;
-    constexpr int kNC = NE >= 8 ? 2 : 1;  // 16-byte query chunks per lane on the byte-row path
+    constexpr int kNC = kU8 ? -NE : (NE >= 8 ? 2 : 1);  // 16-byte query chunks per lane on the byte-row path
     float qreg[(KIND == 0 && NE > 0) ? NE : 1];
     float4 qv[kIntPath ? NE : 1];
-    uint4 qb[kIntPath ? kNC : 1];
+    uint4 qb[(kIntPath || kU8) ? kNC : 1];
+    const float* sqg = sq;  // the query for the generic path (global memory in byte-row instances)
     uint4 qcode[KIND == 1 ? NE : 1];
     bool int_exact = false, u8_mode = false;
     int qq = 0;
@@ -1155,6 +1161,48 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                     }
                 }
             }
+        } else if constexpr (kU8) {
+            qreg[0] = 0.0f;
+            sqg = qg;
+            float lo = INFINITY, hi = -INFINITY;
+            bool integral = true;
+            int s2 = 0;
+            for (int i = lane; i < a.dim; i += 32) {
+                const float v = __ldcg(qg + i);
+                lo = fminf(lo, v);
+                hi = fmaxf(hi, v);
+                integral &= v == rintf(v);
+                if (v >= 0.0f && v <= 255.0f) s2 += (int)v * (int)v;
+            }
+            integral = __all_sync(FULL, integral);
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) {
+                lo = fminf(lo, __shfl_xor_sync(FULL, lo, w));
+                hi = fmaxf(hi, __shfl_xor_sync(FULL, hi, w));
+            }
+            // byte rows hold a base in [0, 255]; a query there too makes every
+            // partial sum an integer below 2^24 (dim <= 256): exact dp4a distances
+            u8_mode = a.u8 != nullptr && integral && lo >= 0.0f && hi <= 255.0f;
+            if (u8_mode) {
+                qq = (int)__reduce_add_sync(FULL, (unsigned)s2);
+#pragma unroll
+                for (int c = 0; c < kNC; ++c) {  // lane t of 8: bytes 16(t + 8c) .. +15
+                    const int e0 = 16 * ((lane & 7) + 8 * c);
+                    unsigned w4[4];
+#pragma unroll
+                    for (int wd = 0; wd < 4; ++wd) {
+                        unsigned wv = 0u;
+#pragma unroll
+                        for (int bt = 0; bt < 4; ++bt) {
+                            const int e = e0 + 4 * wd + bt;
+                            const unsigned bv = e < a.dim ? (unsigned)__ldcg(qg + e) : 0u;
+                            wv |= bv << (8 * bt);
+                        }
+                        w4[wd] = wv;
+                    }
+                    qb[c] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                }
+            }
         } else {
             qreg[0] = 0.0f;
             for (int i = lane; i < a.qdim; i += 32) sq[i] = i < a.dim ? __ldcg(qg + i) : 0.0f;
@@ -1182,6 +1230,9 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
                 if (u8_mode) d = l2_u8<kNC>(a.u8, a.u8_ld, a.u8_ld >> 4, qb, qq, nb, N, rows, lane);
                 else if (int_exact) d = l2_int<NE>(base, a.ld, qv, nb, N, rows, lane);
                 else d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
+            } else if constexpr (kU8) {
+                if (u8_mode) d = l2_u8<kNC>(a.u8, a.u8_ld, a.u8_ld >> 4, qb, qq, nb, N, rows, lane);
+                else d = l2_exact<0>(base, a.ld, a.dim, qreg, sqg, nb, N, lane);
             } else {
                 d = l2_exact<NE>(base, a.ld, a.dim, qreg, sq, nb, N, lane);
             }
@@ -1485,7 +1536,9 @@ template <int KIND, int NE, int GPL, int DT, int LM>
 struct KernelShape {
     static constexpr int kTM = (GPL == 1 && LM == 0) ? 1 : 0;   // result ids in TMEM
     static constexpr int kThreads = GPL == 1 ? 128 : 256;
-    static constexpr int kMinBlocks = GPL == 1 ? ((LM == 1 || LM == 2) ? 4 : 5) : 1;
+    // byte-row instances (NE < 0) hold fewer query registers: 80 per thread, 6 CTAs
+    static constexpr int kMinBlocks =
+        GPL == 1 ? ((LM == 1 || LM == 2) ? 4 : (NE < 0 ? 6 : 5)) : 1;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
 };
 
@@ -1577,6 +1630,10 @@ KernelSel pick_gpl(int kind, const SearchArgs& a) {
     if (kind == SONG_KIND_L2) {
         if (a.prec == SONG_PREC_BF16) return ksel<0, 0, GPL, SONG_PREC_BF16>();
         if (a.prec == SONG_PREC_FP8) return ksel<0, 0, GPL, SONG_PREC_FP8>();
+        if constexpr (GPL == 1) {  // an index with byte rows: the byte-row instances
+            if (a.u8 != nullptr && a.dim <= 128) return ksel<0, -1, 1, 0>();
+            if (a.u8 != nullptr && a.dim <= 256) return ksel<0, -2, 1, 0>();
+        }
         if (a.dim <= 32) return ksel<0, 1, GPL, 0>();
         if (a.dim <= 64) return ksel<0, 2, GPL, 0>();
         if (a.dim <= 128) return ksel<0, 4, GPL, 0>();
@@ -1638,6 +1695,7 @@ template <int LM>
 KernelSel pick_learned(const SearchArgs& a) {
     if (a.prec == SONG_PREC_BF16) return ksel<0, 0, 1, SONG_PREC_BF16, LM>();
     if (a.prec == SONG_PREC_FP8) return ksel<0, 0, 1, SONG_PREC_FP8, LM>();
+    if (a.u8 != nullptr && a.dim <= 128) return ksel<0, -1, 1, 0, LM>();
     if (a.dim <= 128 && a.dim > 64) return ksel<0, 4, 1, 0, LM>();
     return ksel<0, 0, 1, 0, LM>();
 }
