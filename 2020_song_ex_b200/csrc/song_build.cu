@@ -175,6 +175,7 @@ cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim,
         a.dim = dim;
         a.ld = ld;
         a.qld = ld;
+        a.qdim = dim;  // the generic (dim > 256) instance stages this many query floats
         a.block_size = bs;
         a.k = sd;
         a.nq = B;
@@ -299,6 +300,7 @@ cudaError_t build_graph_with_scratch(int kind, const void* d_base, int64_t n, in
         a.dim = dim;
         a.ld = ld;
         a.qld = ld;
+        a.qdim = dim;  // the generic (dim > 256) instance stages this many query floats
         a.block_size = bs;
         a.k = sd;
         a.nq = B;

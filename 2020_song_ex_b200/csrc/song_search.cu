@@ -1536,9 +1536,13 @@ template <int KIND, int NE, int GPL, int DT, int LM>
 struct KernelShape {
     static constexpr int kTM = (GPL == 1 && LM == 0) ? 1 : 0;   // result ids in TMEM
     static constexpr int kThreads = GPL == 1 ? 128 : 256;
-    // byte-row instances (NE < 0) hold fewer query registers: 80 per thread, 6 CTAs
+    // byte-row instances (NE < 0) hold fewer query registers: 80 per thread and 6 CTAs
+    // (plain), 72 and 7 CTAs (learned entry without the stop model), 96 and 5 CTAs
+    // (learned entry and stop)
     static constexpr int kMinBlocks =
-        GPL == 1 ? ((LM == 1 || LM == 2) ? 4 : (NE < 0 ? 6 : 5)) : 1;
+        GPL == 1 ? (LM == 1 ? 4
+                            : (LM == 2 ? (NE < 0 ? 5 : 4) : (NE < 0 ? (LM == 3 ? 7 : 6) : 5)))
+                 : 1;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
 };
 

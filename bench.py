@@ -81,7 +81,7 @@ LEARN_BEAMS = (1, 2, 3, 4)                         # candidates expanded per ste
 LEARN_BLOOM_HASHES = (4, 2)                        # BF_NHASH, and the learned search's cheaper test
 ABLATION_EFS = (64, 72, 80, 88, 96, 112, 128, 160, 192, 256, 320, 384, 512)
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
-METRIC = "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or tensor-core entry + learned models)"
+METRIC = "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or tensor-core entry stage with or without the learned models)"
 DATA = "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)"
 LINE_LIMIT = 4000                                  # bytes of the stdout JSON line
 
@@ -600,14 +600,17 @@ def measure_learned(c, details, plain):
         torch.cuda.synchronize()
         learn_s += time.time() - tl0
         blobs[tef] = song.get_model(g)
-        # threshold 1.0 (entry model only): every beam and Bloom hash count;
-        # learned stop: beams 1, 2 and 4 with 2 hashes
-        for lef, thr, beam, nh in [(e, t, b, h) for e in LEARN_SWEEP_EFS[tef]
-                                   for t in LEARN_THRESHOLDS
-                                   for b in (LEARN_BEAMS if t >= 1.0 else (1, 2, 4))
-                                   for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))]:
+        # threshold 1.0 (no stop): every beam and Bloom hash count, entry points from
+        # the entry model or the entry stage's nearest hubs; learned stop: beams 1, 2
+        # and 4 with 2 hashes and the entry model
+        for lef, thr, beam, nh, ent in [(e, t, b, h, en) for e in LEARN_SWEEP_EFS[tef]
+                                        for t in LEARN_THRESHOLDS
+                                        for b in (LEARN_BEAMS if t >= 1.0 else (1, 2, 4))
+                                        for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))
+                                        for en in ((song.ENTRY_MODEL, song.ENTRY_NEAREST) if t >= 1.0
+                                                   else (song.ENTRY_MODEL,))]:
             opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam,
-                                   bloom_hashes=nh)
+                                   bloom_hashes=nh, entry=ent)
             song.search_device_ex(g, opts, c.dcal, NCAL, K, lef, ids_cal, None, tr_cal, stream=stream)
             stream.synchronize()
             rec = float(ds.recall_at_k(ids_cal.cpu().numpy(), c.gt_cal, K).mean())
@@ -615,7 +618,7 @@ def measure_learned(c, details, plain):
             ms = launch_ms(torch, stream, lambda: song.search_device_ex(
                 g, opts, c.dcal, NCAL, K, lef, ids_cal, None, None, stream=stream))
             lcurve.append({"ef": lef, "trained_ef": tef, "threshold": thr, "beam": beam,
-                           "bloom_hashes": nh, "recall_cal": round(rec, 4),
+                           "bloom_hashes": nh, "entry": ent, "recall_cal": round(rec, 4),
                            "qps": round(NCAL / ms * 1e3),
                            "mean_expanded": round(float(trl[:, 2].mean()), 1),
                            "learned_stop_rate": round(float((trl[:, 11] == 2).mean()), 3)})
@@ -624,14 +627,15 @@ def measure_learned(c, details, plain):
                                          for k2, v in r.items()} for t, r in reps.items()}
     op, reached = choose(lcurve)
     stop_pts = [p for p in lcurve if p["threshold"] < 1.0]
-    nostop_pts = [p for p in lcurve if p["threshold"] >= 1.0]
+    nostop_pts = [p for p in lcurve if p["threshold"] >= 1.0 and p["entry"] == song.ENTRY_MODEL]
     log(f"[rank {c.rank}] learned operating point {op}")
 
-    def opts_of(p, entry=song.ENTRY_MODEL):
+    def opts_of(p, entry=None):
         return song.SearchOpts(precision=prec, learned=True, stop_threshold=p["threshold"],
-                               beam=p["beam"], bloom_hashes=p["bloom_hashes"], entry=entry)
+                               beam=p["beam"], bloom_hashes=p["bloom_hashes"],
+                               entry=p["entry"] if entry is None else entry)
 
-    def evaluate(p, entry=song.ENTRY_MODEL, reps_=5):
+    def evaluate(p, entry=None, reps_=5):
         """Recall, QPS and trace means of point p on the evaluation queries."""
         song.set_model(g, blobs[p["trained_ef"]])
         o = opts_of(p, entry)
@@ -642,7 +646,8 @@ def measure_learned(c, details, plain):
         ms = launch_ms(torch, stream, lambda: song.search_device_ex(
             g, o, c.dq, NQ, K, p["ef"], ids_ev, None, None, stream=stream), reps=reps_)
         return {"ef": p["ef"], "trained_ef": p["trained_ef"], "threshold": p["threshold"],
-                "beam": p["beam"], "bloom_hashes": p["bloom_hashes"], "recall_at_10": round(rec, 4),
+                "beam": p["beam"], "bloom_hashes": p["bloom_hashes"],
+                "entry": p["entry"] if entry is None else entry, "recall_at_10": round(rec, 4),
                 "qps": round(NQ / ms * 1e3), "mean_expanded": round(float(tr[:, 2].mean()), 1),
                 "learned_stop_rate": round(float((tr[:, 11] == 2).mean()), 3)}, tr
 
@@ -669,7 +674,9 @@ def measure_learned(c, details, plain):
         return {"at_target": ev, "at_op_ef": {"ef": op["ef"], "recall_at_10": same_ef["recall_at_10"],
                                               "qps": same_ef["qps"]}}
 
-    ablation = {"no_entry_model": ablate(song.ENTRY_NEAREST),
+    # the same knobs with each entry choice, each at the queue size that reaches the target
+    ablation = {"entry_model": ablate(song.ENTRY_MODEL),
+                "nearest_hubs": ablate(song.ENTRY_NEAREST),
                 "reference_seeds": ablate(song.ENTRY_SEEDS)}
     if stop_pts and nostop_pts:
         bs, oks = choose(stop_pts)
@@ -717,12 +724,14 @@ def measure_learned(c, details, plain):
         e2e = c.ws * NQ * args.steps / timed_host(torch, c.dist, c.ws, dev, args.steps, args.warmup,
                                                   host_learned)
     details["learned_kernel_ms"] = [round(x, 3) for x in kern]
+    entry_name = "learned entry model" if op["entry"] == song.ENTRY_MODEL else "nearest hubs (no model)"
     return {
-        "form": f"tensor-core entry stage ({n_hubs} hubs) + learned entry model"
+        "form": f"tensor-core entry stage ({n_hubs} hubs), {entry_name}"
                 + (" + learned stop" if op["threshold"] < 1.0 else "") + ", byte rows",
-        "kernels": ("entry_kernel + search_kernel<0,4,1,0,3,0> (entry model; the stop cannot fire)"
+        "kernels": ("entry_kernel + search_kernel<0,-1,1,0,3,0> (no stop model)"
                     if op["threshold"] >= 1.0 else
-                    "entry_kernel + search_kernel<0,4,1,0,2,0> (entry + stop models)"),
+                    "entry_kernel + search_kernel<0,-1,1,0,2,0> (stop model)"),
+        "entry": entry_name,
         "threshold": op["threshold"], "beam": op["beam"], "bloom_hashes": op["bloom_hashes"],
         "ef": lef, "trained_ef": op["trained_ef"], "recall_cal": op["recall_cal"],
         "reached_on_calibration": reached,
@@ -759,11 +768,12 @@ def summary_learned(l):
     return {"qps": round(l["qps"], 1), "e2e_qps": round(l["e2e_qps"], 1),
             "recall_at_10": l["recall_at_10"], "ef": l["ef"], "beam": l["beam"],
             "bloom_hashes": l["bloom_hashes"], "stop_threshold": l["threshold"],
-            "learned_stop_rate": l["learned_stop_rate"], "mean_expanded": l["mean_expanded"],
+            "entry": l["entry"], "learned_stop_rate": l["learned_stop_rate"],
+            "mean_expanded": l["mean_expanded"],
             "ablation_qps_recall_ef": {
-                "entry_model": [round(l["qps"]), l["recall_at_10"], l["ef"]],
-                "no_entry_model": short(ab.get("no_entry_model")),
-                "reference_seeds": short(ab.get("reference_seeds")),
+                "entry_model": short(ab.get("entry_model")),
+                "nearest_hubs_no_model": short(ab.get("nearest_hubs")),
+                "reference_seeds_no_entry_stage": short(ab.get("reference_seeds")),
                 "stop_model_on": short(ab.get("stop_model_on")),
                 "stop_model_off": short(ab.get("stop_model_off"))}}
 
