@@ -592,7 +592,11 @@ def measure_learned(c, details, plain):
     tr_cal = c.d_tr[:NCAL]
     lcurve, reps, blobs, learn_s = [], {}, {}, 0.0
     prec = song.PREC_FP32  # the byte rows (exact for these vectors) are read either way
-    for tef in LEARN_EFS:
+    fixed = None
+    if args.learned_fixed:  # profiling cases: one point, no sweep, no ablation
+        f = args.learned_fixed.split(",")
+        fixed = (int(f[0]), float(f[3]), int(f[1]), int(f[2]), int(f[4]))
+    for tef in (LEARN_EFS[:1] if fixed else LEARN_EFS):
         tl0 = time.time()
         reps[tef] = song.learn(g, torch.from_numpy(train).to(dev), ntrain,
                                torch.from_numpy(np.ascontiguousarray(nn1[:, 0])).to(dev),
@@ -603,12 +607,13 @@ def measure_learned(c, details, plain):
         # threshold 1.0 (no stop): every beam and Bloom hash count, entry points from
         # the entry model or the entry stage's nearest hubs; learned stop: beams 1, 2
         # and 4 with 2 hashes and the entry model
-        for lef, thr, beam, nh, ent in [(e, t, b, h, en) for e in LEARN_SWEEP_EFS[tef]
-                                        for t in LEARN_THRESHOLDS
-                                        for b in (LEARN_BEAMS if t >= 1.0 else (1, 2, 4))
-                                        for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))
-                                        for en in ((song.ENTRY_MODEL, song.ENTRY_NEAREST) if t >= 1.0
-                                                   else (song.ENTRY_MODEL,))]:
+        points = [fixed] if fixed else [
+            (e, t, b, h, en) for e in LEARN_SWEEP_EFS[tef]
+            for t in LEARN_THRESHOLDS
+            for b in (LEARN_BEAMS if t >= 1.0 else (1, 2, 4))
+            for h in (LEARN_BLOOM_HASHES if t >= 1.0 else (2,))
+            for en in ((song.ENTRY_MODEL, song.ENTRY_NEAREST) if t >= 1.0 else (song.ENTRY_MODEL,))]
+        for lef, thr, beam, nh, ent in points:
             opts = song.SearchOpts(precision=prec, learned=True, stop_threshold=thr, beam=beam,
                                    bloom_hashes=nh, entry=ent)
             song.search_device_ex(g, opts, c.dcal, NCAL, K, lef, ids_cal, None, tr_cal, stream=stream)
@@ -625,7 +630,7 @@ def measure_learned(c, details, plain):
     details["learned_curve"] = lcurve
     details["learn_reports"] = {str(t): {k2: (round(v, 5) if isinstance(v, float) else v)
                                          for k2, v in r.items()} for t, r in reps.items()}
-    op, reached = choose(lcurve)
+    op, reached = (lcurve[0], True) if fixed else choose(lcurve)
     stop_pts = [p for p in lcurve if p["threshold"] < 1.0]
     nostop_pts = [p for p in lcurve if p["threshold"] >= 1.0 and p["entry"] == song.ENTRY_MODEL]
     log(f"[rank {c.rank}] learned operating point {op}")
@@ -675,10 +680,10 @@ def measure_learned(c, details, plain):
                                               "qps": same_ef["qps"]}}
 
     # the same knobs with each entry choice, each at the queue size that reaches the target
-    ablation = {"entry_model": ablate(song.ENTRY_MODEL),
-                "nearest_hubs": ablate(song.ENTRY_NEAREST),
-                "reference_seeds": ablate(song.ENTRY_SEEDS)}
-    if stop_pts and nostop_pts:
+    ablation = {} if fixed else {"entry_model": ablate(song.ENTRY_MODEL),
+                                 "nearest_hubs": ablate(song.ENTRY_NEAREST),
+                                 "reference_seeds": ablate(song.ENTRY_SEEDS)}
+    if stop_pts and nostop_pts and not fixed:
         bs, oks = choose(stop_pts)
         bn, okn = choose(nostop_pts)
         es, _ = evaluate(bs)
@@ -1303,6 +1308,8 @@ def main(argv=None):
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned form")
+    ap.add_argument("--learned-fixed", default="",
+                    help="profiling cases: one learned point EF,BEAM,HASHES,THRESHOLD,ENTRY (no sweep)")
     ap.add_argument("--no-queue-sweep", action="store_true")
     ap.add_argument("--train-queries", type=int, default=50_000)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
