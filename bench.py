@@ -81,8 +81,8 @@ LEARN_BEAMS = (1, 2, 3, 4)                         # candidates expanded per ste
 LEARN_BLOOM_HASHES = (4, 2)                        # BF_NHASH, and the learned search's cheaper test
 ABLATION_EFS = (64, 72, 80, 88, 96, 112, 128, 160, 192, 256, 320, 384, 512)
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
-METRIC = "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or tensor-core entry stage with or without the learned models)"
-DATA = "synthetic (seeded 1,024-component integer Gaussian mixture; SIFT1M-shaped stand-in)"
+METRIC = "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or the entry-stage/learned form)"
+DATA = "synthetic, seeded (1,024-component integer Gaussian mixture, SIFT1M-shaped)"
 LINE_LIMIT = 4000                                  # bytes of the stdout JSON line
 
 
@@ -198,7 +198,7 @@ def ncu_traffic(ef: int, bf_words: int, form: str = "plain"):
                 c = e.get("config", {})
                 if (c.get("n"), c.get("nq"), c.get("ef"), c.get("bf_words"), c.get("form", "plain")) == \
                         (N_BASE, NQ, ef, bf_words, form):
-                    return e.get("bytes_per_launch_scaled"), e.get("source")
+                    return e.get("bytes_per_launch_scaled"), "profiles/search_kernel_traffic.json (ncu, 1 pass)"
         except (OSError, ValueError):
             pass
     return None, None
@@ -397,9 +397,9 @@ def run_ours(args, ws, rank, local):
                 "graph": graph_src,
                 "storage": "u8 byte rows (base is integer 0-255)" if plain["row_bytes"] < DIM * 4
                            else "fp32 rows",
-                "arithmetic": "exact integer distances equal to the reference's FP32 values",
-                "selection": f"fastest point with recall@10 >= {TARGET_RECALL}+{SELECT_MARGIN} on "
-                             f"{NCAL} calibration queries; reported on the {NQ} evaluation queries",
+                "arithmetic": "exact integer distances (= the reference's FP32 values)",
+                "selection": f"chosen on {NCAL} calibration queries at recall >= "
+                             f"{TARGET_RECALL}+{SELECT_MARGIN}; reported on the evaluation queries",
                 "l2": "inputs larger than L2 (data 512 MB + adj 128 MB per GPU)",
                 "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
             },
@@ -568,10 +568,10 @@ def measure_queue_sweep(c, details, bf_words):
 def summary_queue(q):
     if q is None:
         return None
-    s = {f"k{p['k']}_ef{p['ef']}": [p["qps"], p[f"recall@{p['k']}"]] for p in q["points"]}
-    s["k100_at_0.95"] = {"qps": q["k100"]["qps"], "ef": q["k100"]["ef"],
-                         "recall@100": q["k100"]["recall@100"]}
-    s["cols"] = "qps, recall@k (eval queries)"
+    s = {"cols": "ef, qps, recall@k"}
+    for k in (10, 100):
+        s[f"k{k}"] = [[p["ef"], p["qps"], p[f"recall@{k}"]] for p in q["points"] if p["k"] == k]
+    s["k100_at_target"] = [q["k100"]["ef"], q["k100"]["qps"], q["k100"]["recall@100"]]
     return s
 
 
@@ -846,8 +846,8 @@ def summary_serving(s):
     if s is None:
         return None
     return {"cols": "offered, achieved qps, p50 ms, p99 ms, recall@10",
-            "points": [[p["offered_qps"], p["achieved_qps"], p["p50_ms"], p["p99_ms"],
-                        p.get("recall@10")] for p in s["points"]]}
+            "points": [[p["offered_qps"], round(p["achieved_qps"] or 0), round(p["p50_ms"], 2),
+                        round(p["p99_ms"], 2), p.get("recall@10")] for p in s["points"]]}
 
 
 C3 = {"n": 1_000_000, "dim": 960, "n_comp": 256, "nq": 1000, "seed": 960}
@@ -970,11 +970,9 @@ def measure_c3(c, details):
     details["c3"] = {"forms": res, "curves": curves,
                      "timing_s": {"generate": round(gen_s, 1), "gpu_build": round(build_s, 1)}}
     best = max((v for k2, v in res.items() if k2.endswith("_rerank")), key=lambda v: v["qps"])
-    return {"workload": f"{n} x {dim} L1-normalised 256-comp mixture, {nq} eval queries, deg 31, k=10",
-            "cols": "ef, recall@10, qps, dist rel err max vs fp64",
+    return {"n": n, "cols": "ef, recall@10, qps, max rel dist err vs fp64",
             **{k2: [v["ef"], v["recall_at_10"], v["qps"], v["dist_rel_err_max"]] for k2, v in res.items()},
-            "lowp_rerank_over_fp32": round(best["qps"] / max(res["fp32_plain"]["qps"], 1), 2),
-            "build_s": round(build_s, 1)}
+            "lowp_rerank_over_fp32": round(best["qps"] / max(res["fp32_plain"]["qps"], 1), 2)}
 
 
 def measure_c4(c, details):
@@ -1046,10 +1044,8 @@ def measure_c4(c, details):
     details["c4"] = {"points": out, "curves": curves,
                      "timing_s": {"generate": round(gen_s, 1), "gpu_build": round(build_s, 1),
                                   "learn": round(learn_s, 1)}}
-    return {"workload": f"{n} x {dim} L2-normalised 512-comp anisotropic mixture, {nq} eval queries, deg 31",
-            "cols": "ef, qps, recall@k",
-            **{k2: [v.get("ef"), v.get("qps"), v.get("recall")] for k2, v in out.items()},
-            "build_s": round(build_s, 1)}
+    return {"n": n, "cols": "ef, qps, recall@k",
+            **{k2: [v.get("ef"), v.get("qps"), v.get("recall")] for k2, v in out.items()}}
 
 
 def measure_c4h(c, details):
@@ -1079,9 +1075,8 @@ def measure_c4h(c, details):
         pts.append({"ef": ef, "recall": round(rec, 4), "qps": round(nq / ms * 1e3)})
     g.close()
     details["c4_hamming"] = {"curve": pts, "gpu_build_s": round(build_s, 1)}
-    return {"workload": f"{n} x {dim} -> {bits}-bit codes, {nq} queries, deg 31, k=10",
-            "cols": "ef: qps, recall@10 (vs exact L2 of the vectors)",
-            **{f"ef{p['ef']}": [p["qps"], p["recall"]] for p in pts}, "build_s": round(build_s, 1)}
+    return {"n": n, "cols": "ef, qps, recall@10 vs exact L2 of the vectors",
+            "points": [[p["ef"], p["qps"], p["recall"]] for p in pts]}
 
 
 def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
