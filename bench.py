@@ -853,7 +853,7 @@ def summary_serving(s):
 C3 = {"n": 1_000_000, "dim": 960, "n_comp": 256, "nq": 1000, "seed": 960}
 C4 = {"n": 1_183_514, "dim": 200, "n_comp": 512, "nq": 10_000, "ntrain": 50_000, "seed": 200}
 C4H = {"n": 290_000, "dim": 256, "n_comp": 256, "nq": 10_000, "bits": 512, "seed": 256}
-C3_EFS = (32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024)
+C3_EFS = (32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096)
 C4_EFS = (32, 48, 64, 96, 128, 192, 256, 320, 384, 512, 768, 1024)
 HAM_EFS = (32, 50, 64, 128, 256, 512, 1024)
 
@@ -918,7 +918,7 @@ def measure_c3(c, details):
     cal, ev = m.queries[:nq], m.queries[nq:]
     gt_ev, _ = c.gtm.knn(m.base, ev, K)
     gt_cal, _ = c.gtm.knn(m.base, cal, K)
-    g = song.KernelGraph(n, dim, m.base, song.Params(pq_size=1024, bf_words=512), adj=adj)
+    g = song.KernelGraph(n, dim, m.base, song.Params(pq_size=4096, bf_words=512), adj=adj)
     g.upload_to_gpu()
     dcal, dev_q = torch.from_numpy(cal).to(c.dev), torch.from_numpy(ev).to(c.dev)
     ids_d = torch.empty((nq, K), dtype=torch.int32, device=c.dev)
@@ -957,7 +957,7 @@ def measure_c3(c, details):
         s_bytes = {song.PREC_FP32: dim * 4, song.PREC_BF16: dim * 2, song.PREC_FP8: dim + 4}[prec]
         b = E * s_bytes + X * BLOCK_SIZE * 4 + dim * 4 + K * 4
         if rerank:
-            b = b + np.minimum(op["ef"], 1024) * dim * 4
+            b = b + np.minimum(op["ef"], 4096) * dim * 4
         res[form] = {"ef": op["ef"], "reached_on_calibration": ok, "recall_at_10": round(rec, 4),
                      "qps": round(nq / ms * 1e3), "kernel_ms": round(ms, 4),
                      "dist_rel_err_max": float(f"{rel.max().item():.3e}"),

@@ -179,3 +179,39 @@ def test_concurrent_streams_share_no_buffers(cuda, song, ds):
             torch.cuda.synchronize()
             np.testing.assert_array_equal(torch.cat([o1, o2]).cpu().numpy(), ref.cpu().numpy())
     g.close()
+
+
+def test_entry_choices_are_exact_ablations(cuda, song, ds):
+    """The ablation options change only the entry points: with the
+    reference's seeds (SONG_ENTRY_SEEDS) a learned search without a stop is
+    the plain search, ids and traces bit for bit; with the entry stage's
+    nearest hubs (SONG_ENTRY_NEAREST) it is the seeded search from those
+    hubs."""
+    torch = importlib.import_module("torch")
+    m, g, gt, rep = _setup(song, ds, n=30000, nq=400, ntrain=2000)
+    nq = m.queries.shape[0]
+    tp, ts = song.GpuSearchTrace(), song.GpuSearchTrace()
+    ids_p, _ = song.gpu_search_ex(g, song.SearchOpts(), m.queries, nq, 10, 96, trace=tp)
+    ids_s, _ = song.gpu_search_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0,
+                                                     entry=song.ENTRY_SEEDS),
+                                  m.queries, nq, 10, 96, trace=ts)
+    np.testing.assert_array_equal(ids_s, ids_p)
+    np.testing.assert_array_equal(ts.queries, tp.queries)
+    dq = torch.from_numpy(m.queries).cuda()
+    cid = torch.empty((nq, song.ENTRY_K), dtype=torch.int32, device="cuda")
+    cd = torch.empty((nq, song.ENTRY_K), dtype=torch.float32, device="cuda")
+    song.entry_candidates(g, dq, nq, cid, cd)
+    seeds = cid[:, :4].contiguous()
+    out_n = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+    out_s = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+    tr_n = torch.empty((nq, 12), dtype=torch.int32, device="cuda")
+    tr_s = torch.empty((nq, 12), dtype=torch.int32, device="cuda")
+    song.search_device_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0, entry=song.ENTRY_NEAREST),
+                          dq, nq, 10, 64, out_n, None, tr_n)
+    song.search_device_seeded(g, song.SearchOpts(), dq, nq, 10, 64, seeds, 4, out_s, None, tr_s)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out_n.cpu().numpy(), out_s.cpu().numpy())
+    np.testing.assert_array_equal(tr_n.cpu().numpy(), tr_s.cpu().numpy())
+    with pytest.raises(song.SongError):  # entry choices beyond the three are refused
+        song.gpu_search_ex(g, song.SearchOpts(learned=True, entry=3), m.queries, nq, 10, 64)
+    g.close()
