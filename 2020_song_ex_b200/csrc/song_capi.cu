@@ -77,6 +77,21 @@ struct song_index {
     // allocated on the call's stream and freed on it after the launches that
     // use it, so searches of one index on different streams share no buffer.
     cudaMemPool_t pool = nullptr;
+    // The learned search's entry-stage buffers come from a ring of kEntryRing
+    // persistent slots instead of that pool, so that nothing but kernels sits
+    // between consecutive learned calls on a stream: the entry stage of one
+    // call may then start while the previous call's search finishes its tail.
+    // A slot is reused kEntryRing learned calls later.
+    struct EntrySlot {
+        int32_t* ecand = nullptr;
+        float* edist = nullptr;
+        void* split = nullptr;
+        size_t split_bytes = 0;
+        int cap_nq = 0;
+    };
+    static constexpr int kEntryRing = 16;
+    EntrySlot eslot[kEntryRing];
+    unsigned eslot_next = 0;
     // learned entry / stop models
     bool has_model = false;
     bool model_staged = false;  // the entry model scores the entry stage's candidates
@@ -163,6 +178,11 @@ void free_index(song_index* x) {
     cudaFree(x->d_entry_tiles);
     cudaFree(x->d_entry_norm);
     if (x->pool) cudaMemPoolDestroy(x->pool);  // released once its async frees complete
+    for (auto& sl : x->eslot) {
+        cudaFree(sl.ecand);
+        cudaFree(sl.edist);
+        cudaFree(sl.split);
+    }
     cudaFree(x->d_bf16);
     cudaFree(x->d_fp8);
     cudaFree(x->d_fp8_scale);
@@ -439,19 +459,52 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
     return SONG_OK;
 }
 
+// The next entry-stage ring slot, holding at least nq queries.  Growing a
+// slot (the first calls, or a larger batch) waits for the device first, since
+// a call in flight may still use the old buffers.
+song_status entry_slot(song_index* x, int nq, song_index::EntrySlot** out) {
+    song_index::EntrySlot& sl = x->eslot[x->eslot_next++ % song_index::kEntryRing];
+    if (sl.cap_nq < nq) {
+        SONG_CUDA(cudaDeviceSynchronize(), "entry ring growth");
+        cudaFree(sl.ecand);
+        cudaFree(sl.edist);
+        cudaFree(sl.split);
+        sl = song_index::EntrySlot();
+        const int cap = std::max(nq, 1024);
+        const size_t cells = (size_t)cap * song::kEntryK;
+        const size_t sb = song::entry_split_scratch_bytes(cap, x->num_sms);
+        cudaError_t e = cudaMalloc(&sl.ecand, cells * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&sl.edist, cells * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&sl.split, sb);
+        if (e == cudaSuccess) e = cudaMemset(sl.split, 0, sb);  // arrival counters start at zero
+        if (e != cudaSuccess) {
+            cudaFree(sl.ecand);
+            cudaFree(sl.edist);
+            cudaFree(sl.split);
+            sl = song_index::EntrySlot();
+            return cuda_fail(e, "entry ring slot");
+        }
+        sl.split_bytes = sb;
+        sl.cap_nq = cap;
+    }
+    *out = &sl;
+    return SONG_OK;
+}
+
 song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
-    CallScratch cs(x, st);
     if (a.lm == 2 && x->model_staged && !a.no_entry_stage && a.qseeds == nullptr &&
         a.ecand == nullptr && a.nq > 0) {
-        // learned search: the entry stage first, on the same stream
-        const size_t cells = (size_t)a.nq * song::kEntryK;
-        int32_t* ecand = nullptr;
-        float* edist = nullptr;
-        SONG_CUDA(cs.get(&ecand, cells * 4), "entry candidates alloc");
-        SONG_CUDA(cs.get(&edist, cells * 4), "entry distances alloc");
-        if (song_status s = run_entry(x, a.queries, a.nq, ecand, edist, st)) return s;
-        a.ecand = ecand;
-        a.edist = edist;
+        // learned search: the entry stage first, on the same stream, into a ring
+        // slot; it may overlap the tail of the previous search launch there
+        song_index::EntrySlot* sl = nullptr;
+        if (song_status s = entry_slot(x, a.nq, &sl)) return s;
+        cudaError_t e = song::launch_entry((const float*)a.queries, x->dim, a.nq, x->dim,
+                                           x->d_entry_tiles, x->d_entry_norm, x->d_entry_ids,
+                                           x->entry_hpad, sl->ecand, sl->edist, x->d_err, st,
+                                           sl->split, sl->split_bytes, x->num_sms, true);
+        if (e != cudaSuccess) return cuda_fail(e, "entry launch");
+        a.ecand = sl->ecand;
+        a.edist = sl->edist;
     }
     unsigned* ctr = x->d_counter + 2 * (x->counter_next++ % kCounterRing);
     a.counter = ctr;
@@ -699,6 +752,7 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
         params->fixed_degree > params->block_size || params->search_degree < 1 ||
         params->ef_construction < 1)
         return fail(SONG_ERR_UNSUPPORTED, "GPU build needs 1 <= fixed_degree <= min(32, block_size)");
+    const int ratio = batch_ratio > 0 ? batch_ratio : song::default_batch_ratio(kind, dim);
     const int bfw = build_bf_words > 0 ? build_bf_words : 1024;
     const int ld = song::search_row_stride(kind, dim);
     const song::BaseRange range =
@@ -718,7 +772,7 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
         e = cudaMemcpy2D(d_rows, row_bytes, rows, (size_t)dim * 4, (size_t)dim * 4, (size_t)n,
                          cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-        e = song::build_graph_device(kind, d_rows, n, dim, ld, *params, batch_ratio, bfw, d_adj,
+        e = song::build_graph_device(kind, d_rows, n, dim, ld, *params, ratio, bfw, d_adj,
                                      sms, st, range);
     if (e == cudaSuccess)
         e = cudaMemcpy(adj_out, d_adj, (size_t)n * params->block_size * 4, cudaMemcpyDeviceToHost);

@@ -105,7 +105,8 @@ struct EntryArgs {
     float* out_d;              // [nq x kK]
     float* part_key;           // splits > 1: [splits x nq x kK] keys |h|^2 - 2 q.h
     int32_t* part_idx;         // splits > 1: [splits x nq x kK] hub indices (-1 = none)
-    int* tile_done;            // splits > 1: [query tiles] CTAs finished, zero at launch
+    int* tile_done;            // splits > 1: [query tiles] CTAs finished, zero at launch;
+                               // the merging CTA returns its counter to zero
     int* err;                  // set to 2 when a bounded wait gives up
 };
 
@@ -297,6 +298,7 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
         __syncthreads();
         if (is_last) {
             __threadfence();
+            if (tid == 0) a.tile_done[blockIdx.x] = 0;  // every split has arrived: ready for the next launch
             if (q < a.nq) {
                 // list heads in registers (every split's first entry loaded at once);
                 // each step reloads only the winner's next entry
@@ -350,6 +352,10 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kN)
                      : "memory");
+    // Launched to overlap the previous search launch's tail: this launch ends
+    // only after that one, so work queued after it on the stream also follows
+    // the previous launch (a no-op for an ordinary launch).
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // Hub tiles from FP32 base rows: hub i of the set is node ids[i] (-1 =
@@ -430,7 +436,8 @@ size_t entry_split_scratch_bytes(int nq, int num_sms) {
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
-                         cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms) {
+                         cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms,
+                         bool overlap) {
     if (nq <= 0) return cudaSuccess;
     if (dim > kEntryMaxDim || hpad % kN != 0 || hpad <= 0) return cudaErrorInvalidValue;
     EntryArgs a;
@@ -468,11 +475,22 @@ cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
     cudaError_t e = cudaFuncSetAttribute(entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    if (splits > 1) {
+    if (splits > 1 && !overlap) {
         e = cudaMemsetAsync(a.tile_done, 0, head, st);
         if (e != cudaSuccess) return e;
     }
-    entry_kernel<<<dim3((unsigned)((nq + kM - 1) / kM), (unsigned)splits), 128, smem, st>>>(a);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((nq + kM - 1) / kM), (unsigned)splits);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = overlap ? 1 : 0;
+    e = cudaLaunchKernelEx(&cfg, entry_kernel, a);
+    if (e != cudaSuccess) return e;
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return cudaGetLastError();
 }

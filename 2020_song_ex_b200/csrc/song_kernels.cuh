@@ -100,10 +100,15 @@ cudaError_t build_entry_tables(const float* d_base, int ld, int dim, const int32
 // asynchronous memset on the stream before each launch).
 constexpr int kEntrySplits = 16;
 size_t entry_split_scratch_bytes(int nq, int num_sms);
+// overlap: the scratch's arrival counters are zero (the kernel leaves them
+// so) and the launch may start while the previous search launch on the stream
+// finishes its tail; it ends after that launch.  Otherwise a memset zeroes the
+// counters first and the launch is ordinary.
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
-                         cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms);
+                         cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms,
+                         bool overlap = false);
 
 // Graph::search (graph.h:33-115) bit for bit (song_graphsearch.cu).
 int graph_search_frontier_cap(int ef);
@@ -148,6 +153,13 @@ int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a);
 // Launch the plain search on `stream`: chooses the kernel instance for
 // (kind, dim), the warps per CTA and a persistent grid.  Returns a CUDA error.
 cudaError_t launch_search(int kind, const SearchArgs& a, int num_sms, cudaStream_t stream);
+
+// Batch ratio of the GPU build when the caller passes <= 0: batches of
+// inserted/32 nodes, or inserted/256 above 256 dimensions, where nodes of one
+// batch (which do not see each other) cost measurably more recall.
+inline int default_batch_ratio(int kind, int dim) {
+    return (kind == SONG_KIND_L2 && dim > 256) ? 256 : 32;
+}
 
 // Batched-insertion NSW build over device rows (song_build.cu).
 cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim, int ld,

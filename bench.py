@@ -277,10 +277,14 @@ def timed_host(torch, dist, ws, dev, steps, warmup, call):
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    calls = []
     h0 = time.perf_counter()
     for _ in range(steps):
+        c0 = time.perf_counter()
         call()
+        calls.append(time.perf_counter() - c0)
     dt = time.perf_counter() - h0
+    timed_host.last_calls_ms = [round(x * 1e3, 4) for x in calls]
     rep = importlib.import_module("2020_song_ex_b200.replicas")
     return rep.max_over_ranks(dt, device=dev)
 
@@ -507,6 +511,9 @@ def measure_plain(c, details):
                 raise song.SongError(st, L.song_last_error().decode())
 
         e2e_s = timed_host(torch, c.dist, c.ws, c.dev, args.steps, args.warmup, host_plain)
+        details["plain_e2e_call_ms"] = timed_host.last_calls_ms
+        details["plain_e2e_last_timing"] = {f: round(getattr(timing, f), 4) for f in
+                                            ("h2d_ms", "kernel_ms", "d2h_ms", "total_ms")}
         assert np.array_equal(hids.numpy(), ids_op), "host-API ids differ from the device path"
         e2e = c.ws * NQ * args.steps / e2e_s
     details["plain_curve"] = curve
@@ -728,6 +735,9 @@ def measure_learned(c, details, plain):
 
         e2e = c.ws * NQ * args.steps / timed_host(torch, c.dist, c.ws, dev, args.steps, args.warmup,
                                                   host_learned)
+        details["learned_e2e_call_ms"] = timed_host.last_calls_ms
+        details["learned_e2e_last_timing"] = {f: round(getattr(timing, f), 4) for f in
+                                              ("h2d_ms", "kernel_ms", "d2h_ms", "total_ms")}
     details["learned_kernel_ms"] = [round(x, 3) for x in kern]
     entry_name = "learned entry model" if op["entry"] == song.ENTRY_MODEL else "nearest hubs (no model)"
     return {
@@ -913,7 +923,7 @@ def measure_c3(c, details):
     m = ds.l1_mixture(n, 2 * nq, dim=dim, n_comp=C3["n_comp"], seed=C3["seed"])
     gen_s = time.time() - t0
     t0 = time.time()
-    adj = song.build_graph(m.base, song.Params(block_size=32, fixed_degree=31), batch_ratio=32)
+    adj = song.build_graph(m.base, song.Params(block_size=32, fixed_degree=31))  # ratio 256 above 256-d
     build_s = time.time() - t0
     cal, ev = m.queries[:nq], m.queries[nq:]
     gt_ev, _ = c.gtm.knn(m.base, ev, K)

@@ -91,3 +91,36 @@ def test_more_launches_than_the_counter_ring(cuda, song, index):
     got = out.cpu().numpy()
     for i in range(n_launch):
         np.testing.assert_array_equal(got[i], ref, err_msg=f"launch {i}")
+
+
+def test_learned_back_to_back_through_the_entry_ring(cuda, song, ds, index):
+    """Learned searches take their entry-stage buffers from a ring of 16
+    slots, and each entry stage may start while the previous search finishes:
+    40 calls back to back (the ring wraps twice), alternating two batch
+    sizes, give exactly what each call gives alone; so does a stop model."""
+    torch = cuda
+    gtm = __import__("importlib").import_module("2020_song_ex_b200.groundtruth")
+    m, g = index
+    train = ds.int_mixture(20000, 2000, dim=128, n_comp=32, seed=91, query_seed=92).queries
+    nn1, _ = gtm.knn(m.base, train, 1)
+    song.learn(g, torch.from_numpy(train).cuda(), 2000, torch.from_numpy(nn1[:, 0].copy()).cuda(),
+               song.LearnParams(k=10, ef=64, entry_steps=200, stop_steps=300, entry_hubs=2048))
+    qs = [torch.from_numpy(m.queries[:1500]).cuda(), torch.from_numpy(m.queries[1500:3500]).cuda()]
+    for opts in (song.SearchOpts(learned=True, stop_threshold=1.0, beam=4, bloom_hashes=2,
+                                 entry=song.ENTRY_NEAREST),
+                 song.SearchOpts(learned=True, stop_threshold=0.9, beam=2)):
+        refs = []
+        for q in qs:
+            r = torch.empty((q.shape[0], 10), dtype=torch.int32, device="cuda")
+            song.search_device_ex(g, opts, q, q.shape[0], 10, 64, r, None, None)
+            torch.cuda.synchronize()
+            refs.append(r.cpu().numpy())
+        st = torch.cuda.Stream()
+        outs = [torch.full((qs[i % 2].shape[0], 10), -7, dtype=torch.int32, device="cuda") for i in range(40)]
+        torch.cuda.synchronize()
+        for i in range(40):
+            q = qs[i % 2]
+            song.search_device_ex(g, opts, q, q.shape[0], 10, 64, outs[i], None, None, stream=st)
+        st.synchronize()
+        for i in range(40):
+            np.testing.assert_array_equal(outs[i].cpu().numpy(), refs[i % 2], err_msg=f"call {i}")
