@@ -38,6 +38,14 @@ builder, then Graph::search (graph.h:33-115) timed on all host cores and on
 one core (bench_cpu semantics, bench_cpu.cpp:444-451), at the ef where it
 reaches recall@10 0.95 on the same data.
 
+Extra workloads (``--configs``, all by default; one summary each in the
+line's ``configs``): C3, the precision form on 1M x 960 L1-normalised vectors
+(BF16 and per-vector FP8 rows, FP32 re-rank, distance error against FP64);
+C4, 1,183,514 x 200 angular vectors at k 10 and 100 (plain and entry-stage
+forms, models trained on 50,000 held-out queries); C4's Hamming variant,
+512-bit BitHash codes of 290,000 x 256 vectors.  Their graphs come from the
+GPU builder.
+
 Multi-GPU (torchrun): replicas only -- each rank searches its own 10,000
 queries on its own copy of the graph; no collective on the data path.
 """
@@ -1319,7 +1327,8 @@ def main(argv=None):
     ap.add_argument("--train-queries", type=int, default=50_000)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
-    ap.add_argument("--configs", default="", help="extra workloads, comma separated (c3, c4, c4h)")
+    ap.add_argument("--configs", default="c3,c4,c4h",
+                    help="extra workloads, comma separated (c3, c4, c4h; '' = none)")
     ap.add_argument("--c3-n", type=int, default=0, help="C3 base size (0 = 1,000,000)")
     ap.add_argument("--c4-n", type=int, default=0, help="C4 base size (0 = 1,183,514)")
     ap.add_argument("--n", type=int, default=N_BASE, help="base size (profiling cases)")

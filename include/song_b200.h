@@ -198,10 +198,14 @@ song_status song_graph_search_device(song_index* index, const float* d_queries, 
  * asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).
  * Same clamp and results as song_gpu_search.  Searches of one index may
  * run on different streams at the same time: each launch takes its own work
- * counter (a ring of 1024 per index) and its own scratch (entry-stage lists,
- * Graph::search bitmaps) from the index's stream-ordered memory pool, freed
- * on the launching stream.  Host calls on one index are serialised by a
- * lock.  One thing is shared: the index's error word.  A kernel that meets
+ * counter (a ring of 1024 per index), its own entry-stage lists (learned
+ * searches: a ring of 16 slots per index, so at most 16 learned searches of
+ * one index may be in flight at once) and its own Graph::search bitmaps
+ * (from the index's stream-ordered memory pool, freed on the launching
+ * stream).  Consecutive plain searches on one stream, and a learned search's
+ * entry stage after the previous search on its stream, may overlap that
+ * launch's tail; each writes its results only after the launch before it
+ * has finished.  Host calls on one index are serialised by a lock.  One thing is shared: the index's error word.  A kernel that meets
  * an out-of-range id (a corrupted graph or caller seed) sets it instead of
  * reading out of range, and every host call clears it before its own
  * launches and reports it after them, so with searches of one index running
