@@ -411,12 +411,11 @@ class BitHash:
 
 
 def build_graph(rows, params: Optional[Params] = None, kind: int = KIND_L2,
-                batch_ratio: int = 0, build_bf_words: int = 1024) -> np.ndarray:
+                batch_ratio: int = 32, build_bf_words: int = 1024) -> np.ndarray:
     """NSW adjacency [n, block_size] built on the GPU (song_build_graph).
 
     The reference's insertion algorithm (kernalGraph.h:140-149) run in
-    batches of max(1, inserted/batch_ratio) nodes (0: 32, or 256 above 256
-    dimensions); ``rows`` is FP32
+    batches of max(1, inserted/batch_ratio) nodes; ``rows`` is FP32
     ``[n, dim]`` for KIND_L2 or uint32 codes ``[n, words]`` for KIND_HAMMING.
     """
     params = params or Params()

@@ -459,33 +459,37 @@ song_status make_args(song_index* x, const void* d_q, int nq, int k, int ef, int
     return SONG_OK;
 }
 
-// The next entry-stage ring slot, holding at least nq queries.  Growing a
-// slot (the first calls, or a larger batch) waits for the device first, since
-// a call in flight may still use the old buffers.
+// The next entry-stage ring slot, holding at least nq queries.  A slot too
+// small grows the whole ring at once (the first learned call, or a larger
+// batch): after a device synchronisation, since calls in flight may still use
+// the old buffers.
 song_status entry_slot(song_index* x, int nq, song_index::EntrySlot** out) {
     song_index::EntrySlot& sl = x->eslot[x->eslot_next++ % song_index::kEntryRing];
     if (sl.cap_nq < nq) {
         SONG_CUDA(cudaDeviceSynchronize(), "entry ring growth");
-        cudaFree(sl.ecand);
-        cudaFree(sl.edist);
-        cudaFree(sl.split);
-        sl = song_index::EntrySlot();
-        const int cap = std::max(nq, 1024);
+        int cap = std::max(nq, 1024);
+        for (auto& r : x->eslot) cap = std::max(cap, r.cap_nq);
         const size_t cells = (size_t)cap * song::kEntryK;
         const size_t sb = song::entry_split_scratch_bytes(cap, x->num_sms);
-        cudaError_t e = cudaMalloc(&sl.ecand, cells * 4);
-        if (e == cudaSuccess) e = cudaMalloc(&sl.edist, cells * 4);
-        if (e == cudaSuccess) e = cudaMalloc(&sl.split, sb);
-        if (e == cudaSuccess) e = cudaMemset(sl.split, 0, sb);  // arrival counters start at zero
-        if (e != cudaSuccess) {
-            cudaFree(sl.ecand);
-            cudaFree(sl.edist);
-            cudaFree(sl.split);
-            sl = song_index::EntrySlot();
-            return cuda_fail(e, "entry ring slot");
+        for (auto& r : x->eslot) {
+            cudaFree(r.ecand);
+            cudaFree(r.edist);
+            cudaFree(r.split);
+            r = song_index::EntrySlot();
+            cudaError_t e = cudaMalloc(&r.ecand, cells * 4);
+            if (e == cudaSuccess) e = cudaMalloc(&r.edist, cells * 4);
+            if (e == cudaSuccess) e = cudaMalloc(&r.split, sb);
+            if (e == cudaSuccess) e = cudaMemset(r.split, 0, sb);  // arrival counters start at zero
+            if (e != cudaSuccess) {
+                cudaFree(r.ecand);
+                cudaFree(r.edist);
+                cudaFree(r.split);
+                r = song_index::EntrySlot();
+                return cuda_fail(e, "entry ring slot");
+            }
+            r.split_bytes = sb;
+            r.cap_nq = cap;
         }
-        sl.split_bytes = sb;
-        sl.cap_nq = cap;
     }
     *out = &sl;
     return SONG_OK;
@@ -752,7 +756,7 @@ song_status song_build_graph(int kind, const void* rows, int64_t n, int dim,
         params->fixed_degree > params->block_size || params->search_degree < 1 ||
         params->ef_construction < 1)
         return fail(SONG_ERR_UNSUPPORTED, "GPU build needs 1 <= fixed_degree <= min(32, block_size)");
-    const int ratio = batch_ratio > 0 ? batch_ratio : song::default_batch_ratio(kind, dim);
+    const int ratio = batch_ratio > 0 ? batch_ratio : 32;
     const int bfw = build_bf_words > 0 ? build_bf_words : 1024;
     const int ld = song::search_row_stride(kind, dim);
     const song::BaseRange range =

@@ -154,13 +154,6 @@ int search_warp_smem(int kind, int dim, int cap, int bf_words, SearchArgs* a);
 // (kind, dim), the warps per CTA and a persistent grid.  Returns a CUDA error.
 cudaError_t launch_search(int kind, const SearchArgs& a, int num_sms, cudaStream_t stream);
 
-// Batch ratio of the GPU build when the caller passes <= 0: batches of
-// inserted/32 nodes, or inserted/256 above 256 dimensions, where nodes of one
-// batch (which do not see each other) cost measurably more recall.
-inline int default_batch_ratio(int kind, int dim) {
-    return (kind == SONG_KIND_L2 && dim > 256) ? 256 : 32;
-}
-
 // Batched-insertion NSW build over device rows (song_build.cu).
 cudaError_t build_graph_device(int kind, const void* d_base, int64_t n, int dim, int ld,
                                const song_params& p, int ratio, int bf_words, int32_t* d_adj,

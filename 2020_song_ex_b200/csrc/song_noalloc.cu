@@ -89,7 +89,7 @@ song_status song_build_graph_noalloc(int kind, const void* d_rows, int64_t n, in
         params->ef_construction < 1)
         return song::set_error(SONG_ERR_UNSUPPORTED,
                                "GPU build needs 1 <= fixed_degree <= min(32, block_size)");
-    const int ratio = batch_ratio > 0 ? batch_ratio : song::default_batch_ratio(kind, dim);
+    const int ratio = batch_ratio > 0 ? batch_ratio : 32;
     const int bfw = build_bf_words > 0 ? build_bf_words : 1024;
     const size_t need = song::build_scratch_bytes(n, *params, ratio);
     if (need == (size_t)-1) {

@@ -583,7 +583,7 @@ def measure_queue_sweep(c, details, bf_words):
 def summary_queue(q):
     if q is None:
         return None
-    s = {"cols": "ef, qps, recall@k"}
+    s = {"cols": "ef,qps,recall@k"}
     for k in (10, 100):
         s[f"k{k}"] = [[p["ef"], p["qps"], p[f"recall@{k}"]] for p in q["points"] if p["k"] == k]
     s["k100_at_target"] = [q["k100"]["ef"], q["k100"]["qps"], q["k100"]["recall@100"]]
@@ -863,7 +863,7 @@ def measure_serving(c, details):
 def summary_serving(s):
     if s is None:
         return None
-    return {"cols": "offered, achieved qps, p50 ms, p99 ms, recall@10",
+    return {"cols": "offered,achieved,p50 ms,p99 ms,recall@10",
             "points": [[p["offered_qps"], round(p["achieved_qps"] or 0), round(p["p50_ms"], 2),
                         round(p["p99_ms"], 2), p.get("recall@10")] for p in s["points"]]}
 
@@ -931,7 +931,7 @@ def measure_c3(c, details):
     m = ds.l1_mixture(n, 2 * nq, dim=dim, n_comp=C3["n_comp"], seed=C3["seed"])
     gen_s = time.time() - t0
     t0 = time.time()
-    adj = song.build_graph(m.base, song.Params(block_size=32, fixed_degree=31))  # ratio 256 above 256-d
+    adj = song.build_graph(m.base, song.Params(block_size=32, fixed_degree=31), batch_ratio=32)
     build_s = time.time() - t0
     cal, ev = m.queries[:nq], m.queries[nq:]
     gt_ev, _ = c.gtm.knn(m.base, ev, K)
@@ -988,7 +988,7 @@ def measure_c3(c, details):
     details["c3"] = {"forms": res, "curves": curves,
                      "timing_s": {"generate": round(gen_s, 1), "gpu_build": round(build_s, 1)}}
     best = max((v for k2, v in res.items() if k2.endswith("_rerank")), key=lambda v: v["qps"])
-    return {"n": n, "cols": "ef, recall@10, qps, max rel dist err vs fp64",
+    return {"n": n, "cols": "ef,recall,qps,max rel err vs fp64",
             **{k2: [v["ef"], v["recall_at_10"], v["qps"], v["dist_rel_err_max"]] for k2, v in res.items()},
             "lowp_rerank_over_fp32": round(best["qps"] / max(res["fp32_plain"]["qps"], 1), 2)}
 
@@ -1062,7 +1062,7 @@ def measure_c4(c, details):
     details["c4"] = {"points": out, "curves": curves,
                      "timing_s": {"generate": round(gen_s, 1), "gpu_build": round(build_s, 1),
                                   "learn": round(learn_s, 1)}}
-    return {"n": n, "cols": "ef, qps, recall@k",
+    return {"n": n, "cols": "ef,qps,recall@k",
             **{k2: [v.get("ef"), v.get("qps"), v.get("recall")] for k2, v in out.items()}}
 
 
@@ -1093,7 +1093,7 @@ def measure_c4h(c, details):
         pts.append({"ef": ef, "recall": round(rec, 4), "qps": round(nq / ms * 1e3)})
     g.close()
     details["c4_hamming"] = {"curve": pts, "gpu_build_s": round(build_s, 1)}
-    return {"n": n, "cols": "ef, qps, recall@10 vs exact L2 of the vectors",
+    return {"n": n, "cols": "ef,qps,recall vs exact L2",
             "points": [[p["ef"], p["qps"], p["recall"]] for p in pts]}
 
 
