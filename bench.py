@@ -824,7 +824,10 @@ def measure_serving(c, details):
                song.LearnParams(k=10, ef=max(SERVE_EFS)))
     rng = np.random.default_rng(SEED + c.rank)
     out = []
-    cfg = song.ServerConfig(max_k=max(SERVE_KS), max_ef=max(SERVE_EFS), stop_threshold=0.85)
+    # BF16 rows, the precision form's storage (exact for these integer vectors)
+    song.set_precision(g, song.PREC_BF16)
+    cfg = song.ServerConfig(max_k=max(SERVE_KS), max_ef=max(SERVE_EFS), stop_threshold=0.85,
+                            precision=song.PREC_BF16)
     with song.Server(g, cfg) as srv:
         for rate in SERVE_RATES:
             nreq = int(min(NQ, max(2000, rate * args.serve_seconds)))
@@ -856,7 +859,7 @@ def measure_serving(c, details):
                         "mean_ms": round(float(lat.mean()), 3), **rec, "by_queue": by_ef})
             log(f"[rank {c.rank}] serving {out[-1]}")
     details["serving"] = out
-    return {"form": "learned entry/stop at threshold 0.85, full search when not confident",
+    return {"form": "BF16 rows, learned entry/stop at threshold 0.85, full search when not confident",
             "k_choices": list(SERVE_KS), "queue_choices": list(SERVE_EFS), "points": out}
 
 

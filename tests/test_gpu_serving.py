@@ -130,3 +130,22 @@ def test_idle_wait_runs_out_then_relaunch(cuda, song, setup):
         ids, _, _ = srv.wait(t1, int(ks[40]), timeout_us=30_000_000)
         ids_a, _ = alone(song, g, m.queries[40], ks[40], efs[40], flags[40], 0.85)
         np.testing.assert_array_equal(ids, ids_a)
+
+
+def test_bf16_serving_same_alone_and_in_mix(cuda, song, setup):
+    """The serving loop on BF16 rows (the precision form's storage) with the
+    learned entry/stop: each result equals the same request searched alone
+    with the same options."""
+    m, g, ks, efs, flags = setup
+    song.set_precision(g, song.PREC_BF16)
+    cfg = song.ServerConfig(max_k=100, max_ef=256, stop_threshold=0.85, precision=song.PREC_BF16)
+    n = 200
+    with song.Server(g, cfg) as srv:
+        t0 = srv.submit(m.queries[:n], ks[:n], efs[:n], flags[:n])
+        got = [srv.wait(t0 + i, int(ks[i]), timeout_us=30_000_000) for i in range(n)]
+    for i in range(n):
+        opts = song.SearchOpts(precision=song.PREC_BF16, learned=bool(flags[i]), stop_threshold=0.85)
+        tr = song.GpuSearchTrace()
+        ids, _ = song.gpu_search_ex(g, opts, m.queries[i][None, :], 1, int(ks[i]), int(efs[i]), trace=tr)
+        np.testing.assert_array_equal(got[i][0], ids[0], err_msg=f"request {i}")
+        np.testing.assert_array_equal(got[i][2], tr.queries[0], err_msg=f"trace {i}")
