@@ -102,18 +102,31 @@ __device__ __forceinline__ void tm_st(uint32_t taddr, unsigned v) {
         : "r"(taddr), "r"(v)
         : "memory");
 }
+// Two columns with one wait.
+__device__ __forceinline__ void tm_st2(uint32_t a0, uint32_t a1, unsigned v0, unsigned v1) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%2};\n\t"
+        "tcgen05.st.sync.aligned.32x32b.x1.b32 [%1], {%3};\n\t"
+        "tcgen05.wait::st.sync.aligned;"
+        :
+        : "r"(a0), "r"(a1), "r"(v0), "r"(v1)
+        : "memory");
+}
 
 // Slot queue of capacity <= 1024 * GPL.  Distances live in shared memory;
 // ids live in shared memory (TM = 0) or in the warp's 32 TMEM lanes, one
 // column per group of 32 slots, slot 32g + l at lane l of column tid + g
-// (TM = 1).  The summary of group g (slots 32g .. 32g+31) is held by lane
-// g % 32 in entry g / 32.  Distances are non-negative, so their bit patterns
-// order like the floats.  All scalar fields are warp-uniform.
-template <int GPL, int TM = 0>
+// (TM = 1).  TD = 1 (with TM = 1): the distances too, in the columns from
+// tdd on, laid out like the ids.  The summary of group g (slots 32g ..
+// 32g+31) is held by lane g % 32 in entry g / 32.  Distances are
+// non-negative, so their bit patterns order like the floats.  All scalar
+// fields are warp-uniform.
+template <int GPL, int TM = 0, int TD = 0>
 struct Queue {
-    float* d;
+    float* d;      // TD = 0
     int* id;       // TM = 0
     uint32_t tid;  // TM = 1: TMEM address of group 0's id column
+    uint32_t tdd;  // TD = 1: TMEM address of group 0's distance column
     int sz;
     int cap;
     unsigned xb[GPL], xi[GPL];  // group maximum bits, first slot holding it (NONE = empty)
@@ -127,8 +140,8 @@ struct Queue {
 };
 
 // Id of slot s (warp-uniform s; every lane gets it).
-template <int GPL, int TM>
-__device__ __forceinline__ int q_id(const Queue<GPL, TM>& q, int s) {
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ int q_id(const Queue<GPL, TM, TD>& q, int s) {
     if constexpr (TM) {
         const unsigned r = tm_ld(q.tid + (uint32_t)(s >> 5));
         return (int)__shfl_sync(FULL, r, s & 31);
@@ -138,8 +151,8 @@ __device__ __forceinline__ int q_id(const Queue<GPL, TM>& q, int s) {
 }
 
 // Id of slot s := v (warp-uniform s and v; called by every lane).
-template <int GPL, int TM>
-__device__ __forceinline__ void q_set_id(Queue<GPL, TM>& q, int s, int v, int lane) {
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ void q_set_id(Queue<GPL, TM, TD>& q, int s, int v, int lane) {
     if constexpr (TM) {
         const uint32_t a = q.tid + (uint32_t)(s >> 5);
         unsigned r = tm_ld(a);
@@ -150,11 +163,56 @@ __device__ __forceinline__ void q_set_id(Queue<GPL, TM>& q, int s, int v, int la
     }
 }
 
-template <int GPL, int TM>
-__device__ __forceinline__ void q_init(Queue<GPL, TM>& q, float* d, int* id, uint32_t tid, int cap) {
+// Distance bits of slot s (warp-uniform s; every lane gets them).
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ unsigned q_dbits(const Queue<GPL, TM, TD>& q, int s) {
+    if constexpr (TD) {
+        const unsigned r = tm_ld(q.tdd + (uint32_t)(s >> 5));
+        return __shfl_sync(FULL, r, s & 31);
+    } else {
+        return fbits(q.d[s]);
+    }
+}
+
+// Slot s := (distance bits b, id v) (warp-uniform s, b, v; called by every
+// lane).  TD: both columns read with one wait.
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ void q_set_slot(Queue<GPL, TM, TD>& q, int s, unsigned b, int v, int lane) {
+    if constexpr (TD) {
+        const uint32_t ai = q.tid + (uint32_t)(s >> 5), ad = q.tdd + (uint32_t)(s >> 5);
+        unsigned ri, rd;
+        tm_ld2(ai, ad, ri, rd);
+        if (lane == (s & 31)) {
+            ri = (unsigned)v;
+            rd = b;
+        }
+        tm_st2(ai, ad, ri, rd);
+    } else {
+        if (lane == 0) reinterpret_cast<unsigned*>(q.d)[s] = b;
+        q_set_id(q, s, v, lane);
+    }
+}
+
+// Distance bits of slot s := b (warp-uniform s and b; called by every lane).
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ void q_set_dbits(Queue<GPL, TM, TD>& q, int s, unsigned b, int lane) {
+    if constexpr (TD) {
+        const uint32_t ad = q.tdd + (uint32_t)(s >> 5);
+        unsigned r = tm_ld(ad);
+        if (lane == (s & 31)) r = b;
+        tm_st(ad, r);
+    } else {
+        if (lane == 0) reinterpret_cast<unsigned*>(q.d)[s] = b;
+    }
+}
+
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ void q_init(Queue<GPL, TM, TD>& q, float* d, int* id, uint32_t tid,
+                                       uint32_t tdd, int cap) {
     q.d = d;
     q.id = id;
     q.tid = tid;
+    q.tdd = tdd;
     q.sz = 0;
     q.cap = cap;
     q.cx = false;
@@ -168,11 +226,11 @@ __device__ __forceinline__ void q_init(Queue<GPL, TM>& q, float* d, int* id, uin
 }
 
 // Refresh the summary of group g from the slot array.  MIN: also the minimum.
-template <bool MIN, int GPL, int TM>
-__device__ __forceinline__ void group_update(Queue<GPL, TM>& q, int g, int lane) {
+// `b`: this lane's slot's distance bits (0 if the slot is empty).
+template <bool MIN, int GPL, int TM, int TD>
+__device__ __forceinline__ void group_update_b(Queue<GPL, TM, TD>& q, int g, int lane, unsigned b) {
     const int s = (g << 5) + lane;
     const bool occ = s < q.sz;
-    const unsigned b = occ ? fbits(q.d[s]) : 0u;
     const unsigned mx = __reduce_max_sync(FULL, b);
     const unsigned mxi = __reduce_min_sync(FULL, (occ && b == mx) ? (unsigned)s : NONE);
     unsigned mn = 0xffffffffu, mni = NONE;
@@ -196,9 +254,22 @@ __device__ __forceinline__ void group_update(Queue<GPL, TM>& q, int g, int lane)
     }
 }
 
+template <bool MIN, int GPL, int TM, int TD>
+__device__ __forceinline__ void group_update(Queue<GPL, TM, TD>& q, int g, int lane) {
+    const bool occ = (g << 5) + lane < q.sz;
+    unsigned b;
+    if constexpr (TD) {
+        const unsigned c = tm_ld(q.tdd + (uint32_t)g);
+        b = occ ? c : 0u;
+    } else {
+        b = occ ? fbits(q.d[(g << 5) + lane]) : 0u;
+    }
+    group_update_b<MIN>(q, g, lane, b);
+}
+
 // First slot holding the maximum over [0, sz) (gpuHeap.h:29, :73, :83, :93).
-template <int GPL, int TM>
-__device__ __forceinline__ void root_max(const Queue<GPL, TM>& q, unsigned& mb, unsigned& mi) {
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ void root_max(const Queue<GPL, TM, TD>& q, unsigned& mb, unsigned& mi) {
     unsigned b = 0u, i = NONE;
 #pragma unroll
     for (int r = 0; r < GPL; ++r)
@@ -211,8 +282,8 @@ __device__ __forceinline__ void root_max(const Queue<GPL, TM>& q, unsigned& mb, 
 }
 
 // First slot holding the minimum over [0, sz) (gpuHeap.h:42, :263).
-template <int GPL, int TM>
-__device__ __forceinline__ void root_min(const Queue<GPL, TM>& q, unsigned& mb, unsigned& mi) {
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ void root_min(const Queue<GPL, TM, TD>& q, unsigned& mb, unsigned& mi) {
     unsigned b = 0xffffffffu, i = NONE;
 #pragma unroll
     for (int r = 0; r < GPL; ++r)
@@ -226,15 +297,18 @@ __device__ __forceinline__ void root_min(const Queue<GPL, TM>& q, unsigned& mb, 
 
 // Move the last slot into slot `hole` and shrink (the removal of
 // Candidates::pop_min, Results::pop_worst and drain_best).
-template <bool MIN, int GPL, int TM>
-__device__ __forceinline__ void q_remove(Queue<GPL, TM>& q, int hole, int lane) {
+template <bool MIN, int GPL, int TM, int TD>
+__device__ __forceinline__ void q_remove(Queue<GPL, TM, TD>& q, int hole, int lane) {
     const int last = q.sz - 1;
     __syncwarp();
     if (hole != last) {
-        if (lane == 0) q.d[hole] = q.d[last];
-        if constexpr (TM) {
+        if constexpr (TD) {
+            q_set_slot(q, hole, q_dbits(q, last), q_id(q, last), lane);
+        } else if constexpr (TM) {
+            if (lane == 0) q.d[hole] = q.d[last];
             q_set_id(q, hole, q_id(q, last), lane);
         } else {
+            if (lane == 0) q.d[hole] = q.d[last];
             if (lane == 0) q.id[hole] = q.id[last];
         }
     }
@@ -246,8 +320,8 @@ __device__ __forceinline__ void q_remove(Queue<GPL, TM>& q, int hole, int lane) 
 }
 
 // Maximum and its first slot (gpuHeap.h:29, :73), from the cache when it holds.
-template <int GPL, int TM>
-__device__ __forceinline__ void root_max_c(Queue<GPL, TM>& q, unsigned& mb, unsigned& mi) {
+template <int GPL, int TM, int TD>
+__device__ __forceinline__ void root_max_c(Queue<GPL, TM, TD>& q, unsigned& mb, unsigned& mi) {
     if (!q.cx) {
         root_max(q, q.cxb, q.cxi);
         q.cx = true;
@@ -259,8 +333,9 @@ __device__ __forceinline__ void root_max_c(Queue<GPL, TM>& q, unsigned& mb, unsi
 // Id of slot `hole`, then q_remove(hole): the same queue afterwards, with the
 // TMEM columns of `hole` and of the last slot read once (one wait) instead
 // of once per id access.
-template <bool MIN, int GPL, int TM>
-__device__ __forceinline__ int q_pop(Queue<GPL, TM>& q, int hole, int lane) {
+template <bool MIN, int GPL, int TM, int TD>
+__device__ __forceinline__ int q_pop(Queue<GPL, TM, TD>& q, int hole, int lane) {
+    static_assert(!TD, "pops serve the candidate queue, whose distances are in shared memory");
     if constexpr (!TM) {
         const int id = q.id[hole];
         q_remove<MIN>(q, hole, lane);
@@ -297,8 +372,8 @@ __device__ __forceinline__ int q_pop(Queue<GPL, TM>& q, int hole, int lane) {
 // Returns how many pushes were accepted.  `stage` (32 ints, TM = 1 only)
 // receives the ids in rank order for the column writes of an append.
 // RC: keep the queue's cached maximum (cxb, cxi) current.
-template <bool MIN, bool RC = false, int GPL, int TM>
-__device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, int nb, int lane,
+template <bool MIN, bool RC = false, int GPL, int TM, int TD>
+__device__ __forceinline__ int q_push(Queue<GPL, TM, TD>& q, unsigned N, float d, int nb, int lane,
                                       int* stage) {
     if (N == 0u) return 0;
     const bool mine = (N >> lane) & 1u;
@@ -309,13 +384,31 @@ __device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, in
     if (room > 0) {
         const int a = nm < room ? nm : room;
         if (mine && rank < a) {
-            q.d[q.sz + rank] = d;
+            if constexpr (TD) stage[32 + rank] = (int)fbits(d);
+            else q.d[q.sz + rank] = d;
             if constexpr (TM) stage[rank] = nb;
             else q.id[q.sz + rank] = nb;
         }
         __syncwarp();
         const int g0 = q.sz >> 5, g1 = (q.sz + a - 1) >> 5;
-        if constexpr (TM) {  // slots sz .. sz+a-1 take the staged ids, column by column
+        if constexpr (TD) {  // ids and distances, column by column; each group's summary from its column
+            const int sz0 = q.sz;
+            q.sz += a;
+            for (int g = g0; g <= g1; ++g) {
+                const uint32_t ci = q.tid + (uint32_t)g, cd = q.tdd + (uint32_t)g;
+                unsigned ri, rd;
+                tm_ld2(ci, cd, ri, rd);
+                const int rr = (g << 5) + lane - sz0;
+                if (rr >= 0 && rr < a) {
+                    ri = (unsigned)stage[rr];
+                    rd = (unsigned)stage[32 + rr];
+                }
+                tm_st2(ci, cd, ri, rd);
+                group_update_b<MIN>(q, g, lane, (g << 5) + lane < q.sz ? rd : 0u);
+            }
+            q.sz = sz0;
+            __syncwarp();
+        } else if constexpr (TM) {  // slots sz .. sz+a-1 take the staged ids, column by column
             for (int g = g0; g <= g1; ++g) {
                 const uint32_t col = q.tid + (uint32_t)g;
                 unsigned r = tm_ld(col);
@@ -335,7 +428,8 @@ __device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, in
             }
         }
         q.sz += a;
-        for (int g = g0; g <= g1; ++g) group_update<MIN>(q, g, lane);
+        if constexpr (!TD)
+            for (int g = g0; g <= g1; ++g) group_update<MIN>(q, g, lane);
         acc = a;
     }
     if (nm > room) {
@@ -347,10 +441,23 @@ __device__ __forceinline__ int q_push(Queue<GPL, TM>& q, unsigned N, float d, in
             const int j = __ffs(rest) - 1;
             const float dj = __shfl_sync(FULL, d, j);
             const int nj = __shfl_sync(FULL, nb, j);
-            if (lane == 0) q.d[fi] = dj;
-            q_set_id(q, (int)fi, nj, lane);
-            __syncwarp();
-            group_update<MIN>(q, (int)(fi >> 5), lane);
+            if constexpr (TD) {  // the slot's two columns, then the group's summary from the distance column
+                const int g = (int)(fi >> 5);
+                const uint32_t ci = q.tid + (uint32_t)g, cd = q.tdd + (uint32_t)g;
+                unsigned ri, rd;
+                tm_ld2(ci, cd, ri, rd);
+                if (lane == (int)(fi & 31)) {
+                    ri = (unsigned)nj;
+                    rd = fbits(dj);
+                }
+                tm_st2(ci, cd, ri, rd);
+                group_update_b<MIN>(q, g, lane, (g << 5) + lane < q.sz ? rd : 0u);
+            } else {
+                if (lane == 0) q.d[fi] = dj;
+                q_set_id(q, (int)fi, nj, lane);
+                __syncwarp();
+                group_update<MIN>(q, (int)(fi >> 5), lane);
+            }
             ++acc;
             root_max(q, M, fi);
             rest &= ~(1u << j);
@@ -673,8 +780,8 @@ __device__ __forceinline__ float ham_lane(const uint32_t* __restrict__ base, int
 // Otherwise the extraction is undone and the trims and drains are replayed.
 // `scratch` (TM = 1: at least cap ints of shared memory) holds the slots of
 // the extracted results; with TM = 0 the free candidate id array does.
-template <int GPL, int TM, int TMC>
-__device__ __forceinline__ int finish(Queue<GPL, TM>& res, Queue<GPL, TMC>& cand, int k,
+template <int GPL, int TM, int TD, int TMC>
+__device__ __forceinline__ int finish(Queue<GPL, TM, TD>& res, Queue<GPL, TMC>& cand, int k,
                                       int32_t* out, float* outd, int lane, int* scratch) {
     const int ng = (res.sz + 31) >> 5;
     for (int g = 0; g < ng; ++g) group_update<true>(res, g, lane);
@@ -688,8 +795,8 @@ __device__ __forceinline__ int finish(Queue<GPL, TM>& res, Queue<GPL, TMC>& cand
         if (lane == 0) {
             xv[i] = mb;
             xs[i] = (int)mi;
-            reinterpret_cast<unsigned*>(res.d)[mi] = 0xffffffffu;  // out of every minimum
         }
+        q_set_dbits(res, (int)mi, 0xffffffffu, lane);  // out of every minimum
         __syncwarp();
         group_update<true>(res, (int)(mi >> 5), lane);
     }
@@ -711,7 +818,11 @@ __device__ __forceinline__ int finish(Queue<GPL, TM>& res, Queue<GPL, TMC>& cand
             }
         }
     } else {
-        for (int i = lane; i < take; i += 32) reinterpret_cast<unsigned*>(res.d)[xs[i]] = xv[i];
+        if constexpr (TD) {
+            for (int i = 0; i < take; ++i) q_set_dbits(res, xs[i], xv[i], lane);
+        } else {
+            for (int i = lane; i < take; i += 32) reinterpret_cast<unsigned*>(res.d)[xs[i]] = xv[i];
+        }
         __syncwarp();
         for (int g = 0; g < ng; ++g) group_update<true>(res, g, lane);
         while (res.sz > k) {  // Results::pop_worst
@@ -826,8 +937,8 @@ __device__ __forceinline__ float l2_lowp(const SearchArgs& a, const float* sq, i
 // Precision form, final step: exact FP32 distances of every entry of the
 // results queue (FP32 rows, 8 lanes per row), then the k smallest by
 // (distance, id) in ascending order, -1 padded.
-template <int GPL, int TM, int TMC>
-__device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL, TM>& res,
+template <int GPL, int TM, int TD, int TMC>
+__device__ __forceinline__ int rerank_finish(const SearchArgs& a, Queue<GPL, TM, TD>& res,
                                              Queue<GPL, TMC>& cand, const float* sq, int32_t* out,
                                              float* outd, int lane) {
     const int m = res.sz;
@@ -1058,16 +1169,22 @@ __device__ __forceinline__ unsigned fkey(float x) {
 // (G = ceil(cap / 32) columns); TMC = 1: so do the candidate ids, in the G
 // columns before them.  The per-warp shared-memory layout then has no id
 // array for that queue.
-template <int KIND, int NE, int GPL, int DT, int LM, int TM = 0, int TMC = TM>
+// TR = 0: the per-query trace is not written (a.trace must be null), so its
+// counters are dead code and free their registers.  TD = 1 (TM = TMC = 1):
+// the results queue's distances in TMEM too.
+template <int KIND, int NE, int GPL, int DT, int LM, int TM = 0, int TMC = TM, int TR = 1, int TD = 0>
 __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsigned char* ws,
                                              int lane, uint32_t tbase = 0) {
+    static_assert(!TD || (TM && TMC), "distances in TMEM go with the ids in TMEM");
     Queue<GPL, TMC> cand;
-    Queue<GPL, TM> res;
+    Queue<GPL, TM, TD> res;
+    // this warp's TMEM columns: [candidate ids (TMC)] [result ids (TM)] [result distances (TD)]
     const uint32_t ngrp = (uint32_t)((a.cap + 31) >> 5);
+    const uint32_t tres = tbase + (TMC ? ngrp : 0u);
     q_init(cand, reinterpret_cast<float*>(ws + a.cd_off), reinterpret_cast<int*>(ws + a.ci_off),
-           tbase, a.cap);
+           tbase, 0u, a.cap);
     q_init(res, reinterpret_cast<float*>(ws + a.rd_off), reinterpret_cast<int*>(ws + a.ri_off),
-           tbase + (TMC ? ngrp : 0u), a.cap);
+           tres, tres + ngrp, a.cap);
     uint64_t* bloom = reinterpret_cast<uint64_t*>(ws + a.bl_off);
     float* sq = reinterpret_cast<float*>(ws + a.q_off);
     int* rows = reinterpret_cast<int*>(ws + a.rows_off);
@@ -1507,7 +1624,7 @@ __device__ __forceinline__ void search_query(const SearchArgs& a, int qid, unsig
     else
         tr.result_count = finish(res, cand, a.k, a.out + (int64_t)qid * a.k, outd, lane,
                                  reinterpret_cast<int*>(bloom));
-    if (a.trace != nullptr && lane == 0) a.trace[qid] = tr;
+    if (TR && a.trace != nullptr && lane == 0) a.trace[qid] = tr;
 }
 
 #include "song_serve_kernel.inc"
@@ -1543,13 +1660,17 @@ struct KernelShape {
         GPL == 1 ? (LM == 1 ? 4
                             : (LM == 2 ? (NE < 0 ? 5 : 4) : (NE < 0 ? (LM == 3 ? 7 : 6) : 5)))
                  : 1;
+    // without the trace counters (TR = 0): one more CTA
+    static constexpr int kMinBlocksNT = GPL == 1 && NE < 0 ? kMinBlocks + 1 : kMinBlocks;
     static constexpr bool kQuerySmem = KIND == 0 && NE == 0;  // query kept in shared memory
 };
 
-// TMC = 1 (TM instances only): the candidate ids in TMEM as well.
-template <int KIND, int NE, int GPL, int DT, int LM = 0, int TMC = 0>
+// TMC = 1 (TM instances only): the candidate ids in TMEM as well.  TR = 0:
+// no per-query trace.  TD = 1 (with TMC = 1): the result distances in TMEM.
+template <int KIND, int NE, int GPL, int DT, int LM = 0, int TMC = 0, int TR = 1, int TD = 0>
 __global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads),
-                                  (KernelShape<KIND, NE, GPL, DT, LM>::kMinBlocks))
+                                  (TR ? KernelShape<KIND, NE, GPL, DT, LM>::kMinBlocks
+                                      : KernelShape<KIND, NE, GPL, DT, LM>::kMinBlocksNT))
     search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int TM = KernelShape<KIND, NE, GPL, DT, LM>::kTM;
@@ -1576,7 +1697,7 @@ __global__ void __launch_bounds__((KernelShape<KIND, NE, GPL, DT, LM>::kThreads)
         if (lane == 0) qid = (int)atomicAdd(a.counter, 1u);
         qid = __shfl_sync(FULL, qid, 0);
         if (qid >= a.nq) break;
-        search_query<KIND, NE, GPL, DT, LM, TM, TMC>(a, qid, ws, lane, tbase);
+        search_query<KIND, NE, GPL, DT, LM, TM, TMC, TR, TD>(a, qid, ws, lane, tbase);
     }
     // Every query of this launch has been claimed: a search launched after
     // this one on the stream with programmatic serialization may start on
@@ -1612,6 +1733,10 @@ using KernelFn = void (*)(const SearchArgs);
 struct KernelSel {
     KernelFn fn = nullptr;      // candidate ids in shared memory
     KernelFn fn_tmc = nullptr;  // tm only: the candidate ids in TMEM too
+    KernelFn fn_nt = nullptr;   // byte-row instances: fn and fn_tmc without the trace
+    KernelFn fn_tmc_nt = nullptr;
+    KernelFn fn_tmd = nullptr;  // byte-row plain instances: result distances in TMEM too
+    KernelFn fn_tmd_nt = nullptr;
     int tm = 0;                 // result ids in TMEM (the CTA allocates tensor memory)
     int threads = 256;
     bool query_smem = true;
@@ -1623,6 +1748,14 @@ KernelSel ksel() {
     KernelSel k;
     k.fn = search_kernel<KIND, NE, GPL, DT, LM, 0>;
     if constexpr (S::kTM) k.fn_tmc = search_kernel<KIND, NE, GPL, DT, LM, 1>;
+    if constexpr (NE < 0 && LM != 1) {  // trace-free copies of the hot instances
+        k.fn_nt = search_kernel<KIND, NE, GPL, DT, LM, 0, 0>;
+        if constexpr (S::kTM) {
+            k.fn_tmc_nt = search_kernel<KIND, NE, GPL, DT, LM, 1, 0>;
+            k.fn_tmd = search_kernel<KIND, NE, GPL, DT, LM, 1, 1, 1>;
+            k.fn_tmd_nt = search_kernel<KIND, NE, GPL, DT, LM, 1, 0, 1>;
+        }
+    }
     k.tm = S::kTM;
     k.threads = S::kThreads;
     k.query_smem = S::kQuerySmem;
@@ -1754,17 +1887,28 @@ cudaError_t tm_ctas_per_sm(KernelFn fn, int dev, int warps, size_t dyn_smem, int
 // are in TMEM too][result distances][Bloom filter], the Bloom region being at
 // least cap ints because finish() may keep the extracted slots there once
 // the search is over.
-void tm_layout(int query_floats, bool cand_in_tmem, SearchArgs* a) {
+void tm_layout(int query_floats, bool cand_in_tmem, bool res_d_in_tmem, SearchArgs* a) {
     const int capr = round_up(a->cap, 32);
     a->q_off = 0;
     a->rows_off = round_up(query_floats * 4, 16);
-    a->cd_off = a->rows_off + 128;
-    a->ci_off = cand_in_tmem ? 0 : a->cd_off + capr * 4;
-    a->rd_off = cand_in_tmem ? a->cd_off + capr * 4 : a->ci_off + capr * 4;
+    // the row list doubles as the push stage: 32 ids, and 32 distances when
+    // the result distances are in TMEM
+    a->cd_off = a->rows_off + (res_d_in_tmem ? 256 : 128);
+    int off = a->cd_off + capr * 4;
+    a->ci_off = 0;
+    if (!cand_in_tmem) {
+        a->ci_off = off;
+        off += capr * 4;
+    }
+    a->rd_off = 0;
+    if (!res_d_in_tmem) {
+        a->rd_off = off;
+        off += capr * 4;
+    }
     a->ri_off = 0;
-    a->bl_off = round_up(a->rd_off + capr * 4, 16);
+    a->bl_off = round_up(off, 16);
     a->warp_smem = round_up(a->bl_off + std::max(a->bf_words * 8, capr * 4), 16);
-    a->tm_warp_cols = (cand_in_tmem ? 2 : 1) * (capr / 32);
+    a->tm_warp_cols = ((cand_in_tmem ? 1 : 0) + 1 + (res_d_in_tmem ? 1 : 0)) * (capr / 32);
 }
 
 }  // namespace
@@ -1867,8 +2011,13 @@ cudaError_t launch_serve(const ServeArgs& s, int num_sms, int max_ctas, int rese
 
 cudaError_t launch_search(int kind, const SearchArgs& args, int num_sms, cudaStream_t stream) {
     if (args.nq <= 0) return cudaSuccess;
-    const KernelSel ks = pick_kernel(kind, args);
+    KernelSel ks = pick_kernel(kind, args);
     if (ks.fn == nullptr) return cudaErrorInvalidValue;
+    if (args.trace == nullptr && ks.fn_nt != nullptr) {
+        ks.fn = ks.fn_nt;
+        ks.fn_tmc = ks.fn_tmc_nt;
+        ks.fn_tmd = ks.fn_tmd_nt;
+    }
     KernelFn fn = ks.fn;
     SearchArgs a = args;
     int dev = 0;
@@ -1885,28 +2034,34 @@ cudaError_t launch_search(int kind, const SearchArgs& args, int num_sms, cudaStr
         // The candidate ids go to shared memory unless that costs resident CTAs
         // (large queues and Bloom filters), then to TMEM as well.
         warps = ks.threads / 32;
-        auto shape = [&](bool cand_tm, SearchArgs* s2, int* per_sm) -> cudaError_t {
-            tm_layout(ks.query_smem ? s2->qdim : 0, cand_tm, s2);
+        auto shape = [&](KernelFn f, bool cand_tm, bool res_d_tm, SearchArgs* s2, int* per_sm) -> cudaError_t {
+            tm_layout(ks.query_smem ? s2->qdim : 0, cand_tm, res_d_tm, s2);
             int cols = 32;
             while (cols < s2->tm_warp_cols * (warps / 4)) cols <<= 1;
             s2->tm_cols = cols;
             *per_sm = 0;
             if (cols > 512 || (size_t)warps * s2->warp_smem > (size_t)smem_optin) return cudaSuccess;
-            return tm_ctas_per_sm(cand_tm ? ks.fn_tmc : ks.fn, dev, warps, (size_t)warps * s2->warp_smem,
-                                  cols, per_sm);
+            return tm_ctas_per_sm(f, dev, warps, (size_t)warps * s2->warp_smem, cols, per_sm);
         };
-        SearchArgs a0 = a, a1 = a;
-        int p0 = 0, p1 = 0;
-        e = shape(false, &a0, &p0);
-        if (e == cudaSuccess) e = shape(true, &a1, &p1);
+        // the layout with the most resident CTAs; on a tie the one with fewer
+        // TMEM accesses (ids, then distances, in shared memory)
+        SearchArgs a0 = a, a1 = a, a2 = a;
+        int p0 = 0, p1 = 0, p2 = 0;
+        e = shape(ks.fn, false, false, &a0, &p0);
+        if (e == cudaSuccess) e = shape(ks.fn_tmc, true, false, &a1, &p1);
+        if (e == cudaSuccess && ks.fn_tmd != nullptr) e = shape(ks.fn_tmd, true, true, &a2, &p2);
         if (e != cudaSuccess) return e;
-        if (p1 > p0) {
+        a = a0;
+        tm_per_sm = p0;
+        if (p1 > tm_per_sm) {
             a = a1;
             fn = ks.fn_tmc;
             tm_per_sm = p1;
-        } else {
-            a = a0;
-            tm_per_sm = p0;
+        }
+        if (p2 > tm_per_sm) {
+            a = a2;
+            fn = ks.fn_tmd;
+            tm_per_sm = p2;
         }
         if (tm_per_sm < 1) return cudaErrorInvalidConfiguration;
     } else {

@@ -86,6 +86,28 @@ def test_l2_matches_oracle(cuda, song, ds, oracle, case):
     np.testing.assert_array_equal(tr.queries, otr)
 
 
+@pytest.mark.parametrize("ef,bfw", [(256, 256), (576, 512), (1024, 1024)])
+def test_untraced_search_matches_oracle(cuda, song, ds, oracle, ef, bfw):
+    """Searches without a trace run the trace-free instances (fewer
+    registers, more resident queries), and at large queues and filters the
+    launcher keeps the result distances in TMEM as well: the ids equal the
+    oracle's, as the traced search's do."""
+    base, q = _case(ds, "int", 4000, 100, 128, seed=ef + bfw)
+    adj = knn_graph(base, 32, 31, seed=ef)
+    meta = dict(kind="l2", block_size=32, pq_size=ef, bf_words=bfw, bf_nhash=4,
+                n_multiprobe=4, k=10, ef=ef)
+    a = dict(base=base, queries=q, adj=adj)
+    ids_tr, tr = song_search(song, meta, a)
+    p = song.Params(block_size=32, pq_size=ef, bf_words=bfw, bf_nhash=4, n_multiprobe=4)
+    with song.KernelGraph(base.shape[0], base.shape[1], base, p, adj=adj) as g:
+        g.upload_to_gpu()
+        ids = song.gpu_search(g, q, q.shape[0], 10, 512, ef).reshape(q.shape[0], 10)
+    oids, otr = oracle_run(oracle, meta, a)
+    np.testing.assert_array_equal(ids_tr, oids)
+    np.testing.assert_array_equal(tr.queries, otr)
+    np.testing.assert_array_equal(ids, oids)
+
+
 @pytest.mark.parametrize("words", [1, 3, 8, 16, 32])
 def test_hamming_matches_oracle(cuda, song, oracle, words):
     rng = np.random.default_rng(words)
