@@ -502,10 +502,14 @@ song_status launch(song_index* x, song::SearchArgs a, cudaStream_t st) {
         // slot; it may overlap the tail of the previous search launch there
         song_index::EntrySlot* sl = nullptr;
         if (song_status s = entry_slot(x, a.nq, &sl)) return s;
+        // without the entry model the search takes the nearest n_multiprobe
+        // hubs and reads nothing else of the list
+        const int keep = a.entry_w == nullptr ? std::min(std::max(a.n_multiprobe, 1), song::kEntryK)
+                                              : song::kEntryK;
         cudaError_t e = song::launch_entry((const float*)a.queries, x->dim, a.nq, x->dim,
                                            x->d_entry_tiles, x->d_entry_norm, x->d_entry_ids,
                                            x->entry_hpad, sl->ecand, sl->edist, x->d_err, st,
-                                           sl->split, sl->split_bytes, x->num_sms, true);
+                                           sl->split, sl->split_bytes, x->num_sms, true, keep);
         if (e != cudaSuccess) return cuda_fail(e, "entry launch");
         a.ecand = sl->ecand;
         a.edist = sl->edist;

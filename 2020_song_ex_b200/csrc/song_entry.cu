@@ -110,7 +110,13 @@ struct EntryArgs {
     int* err;                  // set to 2 when a bounded wait gives up
 };
 
+// KK: hubs kept per query (kK for the entry model's features; fewer when the
+// search only takes the nearest few as entry points).  The first KK of the
+// kK output entries are those of a kK-long list, the rest are -1: the same
+// hubs in the same order, at a fraction of the insertion work.
+template <int KK>
 __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
+    static_assert(KK >= 1 && KK <= kK, "KK in [1, kK]");
     extern __shared__ __align__(128) unsigned char smem[];
     // Each thread's 32 keys of the current accumulator chunk (XOR-swizzled by
     // thread, conflict-free), so that only the keys below its threshold are
@@ -176,10 +182,10 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
     __syncthreads();
 
-    float kd[kK];
-    int ki[kK];
+    float kd[KK];
+    int ki[KK];
 #pragma unroll
-    for (int i = 0; i < kK; ++i) {
+    for (int i = 0; i < KK; ++i) {
         kd[i] = INFINITY;
         ki[i] = -1;
     }
@@ -234,7 +240,7 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
             // keys below this thread's current 24th: a 32-bit mask, then the
             // insertion loop visits only those (the warp pays the largest count
             // among its threads, not one pass per key any thread wants)
-            const float thr = kd[kK - 1];
+            const float thr = kd[KK - 1];
             float dv[32];
             unsigned m = 0u;
 #pragma unroll
@@ -250,10 +256,10 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
                 const int j = __ffs(m) - 1;
                 m &= m - 1u;
                 const float d = my[j ^ sw];
-                if (d < kd[kK - 1]) {  // sorted insertion; equal keys keep the earlier hub first
+                if (d < kd[KK - 1]) {  // sorted insertion; equal keys keep the earlier hub first
                     const int idx = t * kN + c0 + j;
 #pragma unroll
-                    for (int i = kK - 1; i > 0; --i) {
+                    for (int i = KK - 1; i > 0; --i) {
                         const bool shift = d < kd[i - 1];
                         const bool here = !shift && d < kd[i];
                         kd[i] = shift ? kd[i - 1] : (here ? d : kd[i]);
@@ -273,16 +279,22 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     if (q < a.nq) {
         if (gridDim.y > 1) {  // partial list of this split, merged below by the tile's last CTA
             const size_t o = ((size_t)blockIdx.y * a.nq + q) * kK;
-            for (int i = 0; i < kK; ++i) {
+#pragma unroll
+            for (int i = 0; i < KK; ++i) {
                 const bool v = ok && ki[i] >= 0 && kd[i] < INFINITY;
                 a.part_key[o + i] = v ? kd[i] : INFINITY;
                 a.part_idx[o + i] = v ? ki[i] : -1;
             }
         } else {
-            for (int i = 0; i < kK; ++i) {
+#pragma unroll
+            for (int i = 0; i < KK; ++i) {
                 const bool v = ok && ki[i] >= 0 && kd[i] < INFINITY;
                 a.out_ids[(size_t)q * kK + i] = v ? __ldg(a.hub_ids + ki[i]) : -1;
                 a.out_d[(size_t)q * kK + i] = v ? fmaxf(qn + kd[i], 0.0f) : INFINITY;
+            }
+            for (int i = KK; i < kK; ++i) {
+                a.out_ids[(size_t)q * kK + i] = -1;
+                a.out_d[(size_t)q * kK + i] = INFINITY;
             }
         }
     }
@@ -316,7 +328,7 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
                         hk[sp] = __ldcg(a.part_key + o);
                     }
                 }
-                for (int i = 0; i < kK; ++i) {
+                for (int i = 0; i < KK; ++i) {
                     float bk = INFINITY;
                     int bi = INT_MAX, bs = -1;
 #pragma unroll
@@ -335,13 +347,17 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
                             ++pos[sp];
                             hx[sp] = -1;
                             hk[sp] = INFINITY;
-                            if (pos[sp] < kK) {
+                            if (pos[sp] < KK) {
                                 const size_t o = ((size_t)sp * a.nq + q) * kK + pos[sp];
                                 hx[sp] = __ldcg(a.part_idx + o);
                                 hk[sp] = __ldcg(a.part_key + o);
                             }
                         }
                     }
+                }
+                for (int i = KK; i < kK; ++i) {
+                    a.out_ids[(size_t)q * kK + i] = -1;
+                    a.out_d[(size_t)q * kK + i] = INFINITY;
                 }
             }
         }
@@ -437,7 +453,7 @@ cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
                          cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms,
-                         bool overlap) {
+                         bool overlap, int keep) {
     if (nq <= 0) return cudaSuccess;
     if (dim > kEntryMaxDim || hpad % kN != 0 || hpad <= 0) return cudaErrorInvalidValue;
     EntryArgs a;
@@ -472,8 +488,8 @@ cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                                             (size_t)splits * nq * kK * 4);
     a.err = d_err;
     const size_t smem = entry_smem_bytes(dim);
-    cudaError_t e = cudaFuncSetAttribute(entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    void (*kern)(const EntryArgs) = keep <= 4 ? entry_kernel<4> : (keep <= 8 ? entry_kernel<8> : entry_kernel<kK>);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (splits > 1 && !overlap) {
         e = cudaMemsetAsync(a.tile_done, 0, head, st);
@@ -489,7 +505,7 @@ cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = overlap ? 1 : 0;
-    e = cudaLaunchKernelEx(&cfg, entry_kernel, a);
+    e = cudaLaunchKernelEx(&cfg, kern, a);
     if (e != cudaSuccess) return e;
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return cudaGetLastError();

@@ -104,11 +104,14 @@ size_t entry_split_scratch_bytes(int nq, int num_sms);
 // so) and the launch may start while the previous search launch on the stream
 // finishes its tail; it ends after that launch.  Otherwise a memset zeroes the
 // counters first and the launch is ordinary.
+// keep: how many of the nearest hubs the caller reads (the rest of each
+// kEntryK row is -1 / +inf); the first `keep` entries are those of the full
+// list.  kEntryK for the entry model's features.
 cudaError_t launch_entry(const float* d_queries, int qld, int nq, int dim,
                          const __nv_bfloat16* d_tiles, const float* d_norm, const int32_t* d_ids,
                          int hpad, int32_t* d_out_ids, float* d_out_d, int* d_err,
                          cudaStream_t st, void* split_scratch, size_t split_bytes, int num_sms,
-                         bool overlap = false);
+                         bool overlap = false, int keep = kEntryK);
 
 // Graph::search (graph.h:33-115) bit for bit (song_graphsearch.cu).
 int graph_search_frontier_cap(int ef);

@@ -215,3 +215,34 @@ def test_entry_choices_are_exact_ablations(cuda, song, ds):
     with pytest.raises(song.SongError):  # entry choices beyond the three are refused
         song.gpu_search_ex(g, song.SearchOpts(learned=True, entry=3), m.queries, nq, 10, 64)
     g.close()
+
+
+def test_nearest_entry_keeps_the_nearest_hubs(cuda, song, ds):
+    """Without the entry model the entry stage keeps only the n_multiprobe
+    nearest hubs per query (less insertion work); they are the head of the
+    full 24-hub list, at every split of the hub tiles over CTAs (16 splits
+    at 400 queries, 3 at 10,000, 1 at 40,000), so the search from them is
+    the seeded search from that head."""
+    torch = importlib.import_module("torch")
+    m, g, gt, rep = _setup(song, ds, n=30000, nq=400, ntrain=2000)
+    for reps in (1, 25, 100):
+        q = np.ascontiguousarray(np.tile(m.queries, (reps, 1)))
+        nq = q.shape[0]
+        dq = torch.from_numpy(q).cuda()
+        cid = torch.empty((nq, song.ENTRY_K), dtype=torch.int32, device="cuda")
+        cd = torch.empty((nq, song.ENTRY_K), dtype=torch.float32, device="cuda")
+        song.entry_candidates(g, dq, nq, cid, cd)
+        seeds = cid[:, :4].contiguous()
+        out_n = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+        out_s = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+        song.search_device_ex(g, song.SearchOpts(learned=True, stop_threshold=1.0,
+                                                 entry=song.ENTRY_NEAREST),
+                              dq, nq, 10, 64, out_n, None, None)
+        song.search_device_seeded(g, song.SearchOpts(), dq, nq, 10, 64, seeds, 4, out_s, None, None)
+        torch.cuda.synchronize()
+        a_n, a_s = out_n.cpu().numpy(), out_s.cpu().numpy()
+        np.testing.assert_array_equal(a_n, a_s)
+        # every copy of a query found the same neighbours
+        np.testing.assert_array_equal(a_n.reshape(reps, 400, 10),
+                                      np.broadcast_to(a_n[:400], (reps, 400, 10)))
+    g.close()
