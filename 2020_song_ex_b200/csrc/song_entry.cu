@@ -9,8 +9,9 @@
 //     into shared memory (operand B), double buffered so that the next
 //     tile's copy overlaps this tile's work;
 //   * one thread issues K/16 tcgen05.mma (kind::f16, BF16 x BF16 -> FP32,
-//     M = 128, N = 128) into a 128-column TMEM accumulator and commits them
-//     to an mbarrier;
+//     M = 128, N = 128) into one half of a 256-column TMEM accumulator and
+//     commits them to that half's mbarrier, one tile ahead of the warps that
+//     read the other half;
 //   * every thread reads its query's row of the accumulator (tcgen05.ld,
 //     lane = query) and keeps the kEntryK hubs of smallest |h|^2 - 2 q.h in
 //     registers (|q|^2 is the same for every hub of a query).
@@ -48,6 +49,8 @@ constexpr int kM = 128;           // queries per CTA (MMA M)
 constexpr int kN = 128;           // hubs per tile (MMA N), TMEM columns of the accumulator
 constexpr int kK = kEntryK;       // nearest hubs kept per query
 constexpr long long kWaitNs = 2000000000LL;
+
+__device__ __forceinline__ int lane_of(int tid) { return tid & 31; }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -124,7 +127,7 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     __shared__ float stage[kM * 32];
     __shared__ float hn_s[kN];
     __shared__ __align__(8) uint64_t bar_load[2];
-    __shared__ __align__(8) uint64_t bar_mma;
+    __shared__ __align__(8) uint64_t bar_mma[2];
     __shared__ uint32_t tslot;
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t a_bytes = (uint32_t)kM * a.kp * 2, b_bytes = (uint32_t)kN * a.kp * 2;
@@ -134,13 +137,14 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_addr(&tslot)), "r"(kN) : "memory");
+                     :: "r"(smem_addr(&tslot)), "r"(2 * kN) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_load[0])) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_load[1])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_mma)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_mma[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar_mma[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -165,19 +169,38 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
         if (t_begin + 1 < t_end) issue_load(t_begin + 1, 1);
     }
 
-    // operand A: this thread's query as BF16, and its FP32 squared norm
+    // operand A: this thread's query as BF16, and its FP32 squared norm.  The
+    // rows pass through `stage` 32 columns at a time: warp w loads its own 32
+    // rows with one coalesced 128-byte read per row, then every thread converts
+    // its row and sums its squares in increasing k (XOR-swizzled slots keep both
+    // steps free of bank conflicts).
     const int q = blockIdx.x * kM + tid;
     float qn = 0.0f;
-    for (int k0 = 0; k0 < a.kp; k0 += 8) {
-        __align__(16) __nv_bfloat16 v[8];
+    {
+        float* my = stage + tid * 32;
+        const int sw = tid & 31;
+        for (int k0 = 0; k0 < a.kp; k0 += 32) {
+            const int k = k0 + lane_of(tid);
+#pragma unroll 8
+            for (int r = 0; r < 32; ++r) {
+                const int row = warp * 32 + r;
+                const int qr = blockIdx.x * kM + row;
+                const float x = (qr < a.nq && k < a.dim) ? __ldg(a.queries + (size_t)qr * a.qld + k) : 0.0f;
+                stage[row * 32 + (lane_of(tid) ^ r)] = x;
+            }
+            __syncwarp();
+            for (int j0 = 0; j0 < 32 && k0 + j0 < a.kp; j0 += 8) {
+                __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int k = k0 + e;
-            const float x = (q < a.nq && k < a.dim) ? a.queries[(size_t)q * a.qld + k] : 0.0f;
-            qn = fmaf(x, x, qn);
-            v[e] = __float2bfloat16_rn(x);
+                for (int e = 0; e < 8; ++e) {
+                    const float x = my[(j0 + e) ^ sw];
+                    qn = fmaf(x, x, qn);
+                    v[e] = __float2bfloat16_rn(x);
+                }
+                *reinterpret_cast<uint4*>(As + tile_off(tid, k0 + j0, a.kp)) = *reinterpret_cast<const uint4*>(v);
+            }
+            __syncwarp();
         }
-        *reinterpret_cast<uint4*>(As + tile_off(tid, k0, a.kp)) = *reinterpret_cast<const uint4*>(v);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
     __syncthreads();
@@ -189,37 +212,60 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
         kd[i] = INFINITY;
         ki[i] = -1;
     }
-    bool ok = true;
-    for (int t = t_begin; t < t_end; ++t) {
-        const int u = t - t_begin;  // this CTA's u-th tile: buffer u % 2, its (u / 2)-th use
+    // One tile ahead: the MMAs of tile u + 1 run into the other half of the
+    // accumulator (TMEM columns kN * ((u + 1) % 2) ..) while the warps read
+    // tile u; each half completes on its own mbarrier.  lw / mw: loads and MMA
+    // groups waited for (uniform); li / mi: issued (thread 0).
+    auto issue_mma = [&](int u) {
         const int buf = u & 1;
-        // a wait that gives up in any thread ends the loop in every thread
-        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_load[buf]), (uint32_t)((u >> 1) & 1)));
-        if (!ok) break;
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs[buf]);
-            for (int s = 0; s < a.kp / 16; ++s) {
-                const uint64_t ad = umma_desc(a0 + (uint32_t)s * 256u, 128u, sbo);
-                const uint64_t bd = umma_desc(b0 + (uint32_t)s * 256u, 128u, sbo);
-                const uint32_t acc = s > 0 ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                    :: "r"(tmem), "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc) : "memory");
-            }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs[buf]);
+        const uint32_t acc_t = tmem + (uint32_t)(buf * kN);
+        for (int s = 0; s < a.kp / 16; ++s) {
+            const uint64_t ad = umma_desc(a0 + (uint32_t)s * 256u, 128u, sbo);
+            const uint64_t bd = umma_desc(b0 + (uint32_t)s * 256u, 128u, sbo);
+            const uint32_t acc = s > 0 ? 1u : 0u;
             asm volatile(
-                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                :: "r"(smem_addr(&bar_mma)) : "memory");
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                :: "r"(acc_t), "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc) : "memory");
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+            :: "r"(smem_addr(&bar_mma[buf])) : "memory");
+    };
+    const int nt = t_end - t_begin;
+    int lw = 0, mw = 0, li = nt < 2 ? nt : 2, mi = 0;
+    bool ok = true;
+    if (nt > 0) {  // a wait that gives up in any thread ends the work in every thread
+        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_load[0]), 0u));
+        if (ok) {
+            lw = 1;
+            if (tid == 0) issue_mma(0);
+            mi = 1;
+        }
+    }
+    for (int u = 0; ok && u < nt; ++u) {
+        const int t = t_begin + u;  // this CTA's u-th tile: buffers u % 2, their (u / 2)-th use
+        if (u + 1 < nt) {
+            ok = __syncthreads_and(mbar_wait(smem_addr(&bar_load[(u + 1) & 1]), (uint32_t)(((u + 1) >> 1) & 1)));
+            if (!ok) break;
+            lw = u + 2;
+            if (tid == 0) issue_mma(u + 1);
+            mi = u + 2;
         }
         hn_s[tid] = __ldg(a.hub_norm + (size_t)t * kN + tid);  // kN == blockDim.x
-        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_mma), (uint32_t)(u & 1)));
+        ok = __syncthreads_and(mbar_wait(smem_addr(&bar_mma[u & 1]), (uint32_t)((u >> 1) & 1)));
         if (!ok) break;
+        mw = u + 1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // the MMAs have read this buffer: refill it with tile t + 2
-        if (tid == 0 && t + 2 < t_end) issue_load(t + 2, buf);
-        const uint32_t row = tmem + ((uint32_t)(warp * 32) << 16);
+        // the MMAs of tile u have read its buffer: refill it with tile u + 2
+        if (tid == 0 && u + 2 < nt) {
+            issue_load(t + 2, u & 1);
+            ++li;
+        }
+        const uint32_t row = tmem + (uint32_t)((u & 1) * kN) + ((uint32_t)(warp * 32) << 16);
         float* my = stage + tid * 32;
         const int sw = tid & 31;
         for (int c0 = 0; c0 < kN; c0 += 32) {
@@ -273,9 +319,18 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();  // every warp has read the accumulator before the next MMA
+        __syncthreads();  // every warp has read this half before its next MMA
     }
-    if (!ok && tid == 0) atomicExch(a.err, 2);
+    if (!ok) {
+        // the copies and MMAs still in flight land before the CTA frees its
+        // shared and tensor memory (each wait again bounded)
+        if (tid == 0) {
+            atomicExch(a.err, 2);
+            for (int v = lw; v < li; ++v) mbar_wait(smem_addr(&bar_load[v & 1]), (uint32_t)((v >> 1) & 1));
+            for (int v = mw; v < mi; ++v) mbar_wait(smem_addr(&bar_mma[v & 1]), (uint32_t)((v >> 1) & 1));
+        }
+        __syncthreads();
+    }
     if (q < a.nq) {
         if (gridDim.y > 1) {  // partial list of this split, merged below by the tile's last CTA
             const size_t o = ((size_t)blockIdx.y * a.nq + q) * kK;
@@ -366,7 +421,7 @@ __global__ void __launch_bounds__(128, 1) entry_kernel(const EntryArgs a) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kN)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(2 * kN)
                      : "memory");
     // Launched to overlap the previous search launch's tail: this launch ends
     // only after that one, so work queued after it on the stream also follows
