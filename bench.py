@@ -87,6 +87,10 @@ LEARN_EFS = (96, 160)                              # queue sizes the models are 
 LEARN_SWEEP_EFS = {96: (64, 72, 80, 88, 96, 128), 160: (160, 192, 256)}
 LEARN_BEAMS = (1, 2, 3, 4)                         # candidates expanded per step
 LEARN_BLOOM_HASHES = (4, 2)                        # BF_NHASH, and the learned search's cheaper test
+# The learned form's own Bloom filter: its searches insert about 69 x 31 ids, 1.5 % false
+# positives with 2 hashes in 32,768 bits; a larger filter (the plain form's choice may be
+# 1,024 words) would only cost resident warps (8 KB of shared memory per query instead of 4).
+LEARN_BF_WORDS = 512
 ABLATION_EFS = (64, 72, 80, 88, 96, 112, 128, 160, 192, 256, 320, 384, 512)
 WORKLOAD = "plain-L2 1M x 128 int-mixture(1024 comps), 10k queries, NSW deg 31 (BLOCK_SIZE 32), k=10"
 METRIC = "QPS at recall@10>=0.95 (fastest form: plain bit-exact, or the entry-stage/learned form)"
@@ -365,9 +369,16 @@ def run_ours(args, ws, rank, local):
     plain = measure_plain(c, details)
     c.g = plain.pop("_graph")
     queue = measure_queue_sweep(c, details, plain["bf_words"]) if not args.no_queue_sweep else None
+    c.gl = None
+    if not args.no_learned:  # the learned form's index: the same rows and graph, its own filter size
+        c.gl = song.KernelGraph(N_BASE, DIM, c.base, song.Params(pq_size=1024, bf_words=LEARN_BF_WORDS),
+                                adj=c.adj)
+        c.gl.upload_to_gpu()
     learned = None if args.no_learned else measure_learned(c, details, plain)
     serving = None if args.no_serving else measure_serving(c, details)
     c.g.close()
+    if c.gl is not None:
+        c.gl.close()
 
     out = None
     if rank == 0:
@@ -381,7 +392,7 @@ def run_ours(args, ws, rank, local):
         roof_learned = None
         if learned is not None and "qps" in learned:
             roof_learned = roofline(learned, peak, peak_kind, learned["kernels"],
-                                    ncu_traffic(learned["ef"], plain["bf_words"], form="learned"))
+                                    ncu_traffic(learned["ef"], LEARN_BF_WORDS, form="learned"))
         best = learned if use_learned else plain
         details.update({"plain": strip(plain), "learned": strip(learned), "queue_sweep": queue,
                         "serving": serving, "cpu_baseline": cpu, "reference_gpu_kernel": refgpu,
@@ -404,7 +415,7 @@ def run_ours(args, ws, rank, local):
             "config": {
                 "workload": WORKLOAD, "n": N_BASE, "dim": DIM, "nq_per_gpu": NQ, "k": K,
                 "form": "learned" if use_learned else "plain",
-                "ef": best["ef"], "bf_words": plain["bf_words"],
+                "ef": best["ef"], "bf_words": LEARN_BF_WORDS if use_learned else plain["bf_words"],
                 "bloom_hashes": best.get("bloom_hashes", 4), "beam": best.get("beam", 1),
                 "graph": graph_src,
                 "storage": "u8 byte rows (base is integer 0-255)" if plain["row_bytes"] < DIM * 4
@@ -472,7 +483,7 @@ def measure_plain(c, details):
         for ef in efs:
             ids_v = d_ids[:NCAL]
             ms = launch_ms(torch, stream, lambda: song.search_device(g, c.dcal, NCAL, K, ef, ids_v, None,
-                                                                     stream=stream), reps=1)
+                                                                     stream=stream), reps=3)
             rec = float(ds.recall_at_k(ids_v.cpu().numpy(), c.gt_cal, K).mean())
             curve.append({"ef": ef, "bf_words": bfw, "recall_cal": round(rec, 4),
                           "qps": round(NCAL / ms * 1e3)})
@@ -597,7 +608,7 @@ def measure_learned(c, details, plain):
     torch, song, ds, gtm, args = c.torch, c.song, c.ds, c.gtm, c.args
     import ctypes as C
     L = song.load_library()
-    g, stream, dev = c.g, c.stream, c.dev
+    g, stream, dev = c.gl, c.stream, c.dev
     ntrain = args.train_queries
     train = draw_queries(ntrain, TRAIN_SEED + c.rank)
     nn1, _ = gtm.knn(c.base, train, 1)
@@ -756,6 +767,7 @@ def measure_learned(c, details, plain):
                     "entry_kernel + search_kernel<0,-1,1,0,2,0> (stop model)"),
         "entry": entry_name,
         "threshold": op["threshold"], "beam": op["beam"], "bloom_hashes": op["bloom_hashes"],
+        "bf_words": LEARN_BF_WORDS,
         "ef": lef, "trained_ef": op["trained_ef"], "recall_cal": op["recall_cal"],
         "reached_on_calibration": reached,
         "qps": c.ws * NQ * args.steps / (total_ms / 1e3),
@@ -790,7 +802,7 @@ def summary_learned(l):
 
     return {"qps": round(l["qps"], 1), "e2e_qps": round(l["e2e_qps"], 1),
             "recall_at_10": l["recall_at_10"], "ef": l["ef"], "beam": l["beam"],
-            "bloom_hashes": l["bloom_hashes"], "stop_threshold": l["threshold"],
+            "bloom_hashes": l["bloom_hashes"], "bf_words": l.get("bf_words"), "stop_threshold": l["threshold"],
             "entry": l["entry"], "learned_stop_rate": l["learned_stop_rate"],
             "mean_expanded": l["mean_expanded"],
             "ablation_qps_recall_ef": {
