@@ -102,7 +102,8 @@ struct song_index {
     __half* d_stop_w = nullptr;
     int ckpt_every = 8, min_expansions = 8, model_k = 10;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_h = nullptr, ev_d = nullptr;  // host-call timing
+    int* h_err = nullptr;  // pinned host copy of the error word for host calls
     std::mutex mu;
 };
 
@@ -191,6 +192,9 @@ void free_index(song_index* x) {
     cudaFree(x->d_stop_w);
     if (x->ev0) cudaEventDestroy(x->ev0);
     if (x->ev1) cudaEventDestroy(x->ev1);
+    if (x->ev_h) cudaEventDestroy(x->ev_h);
+    if (x->ev_d) cudaEventDestroy(x->ev_d);
+    if (x->h_err) cudaFreeHost(x->h_err);
     if (x->stream) cudaStreamDestroy(x->stream);
     cudaSetDevice(cur);
     delete x;
@@ -240,6 +244,9 @@ song_status create_common(int kind, const void* rows, int64_t n, int dim, const 
     }
     if (e == cudaSuccess) e = cudaEventCreate(&x->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&x->ev1);
+    if (e == cudaSuccess) e = cudaEventCreate(&x->ev_h);
+    if (e == cudaSuccess) e = cudaEventCreate(&x->ev_d);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&x->h_err, sizeof(int), cudaHostAllocDefault);
     if (e == cudaSuccess && x->ld != dim) e = cudaMemset(x->d_base, 0, (size_t)n * row_bytes);
     if (e == cudaSuccess)
         e = cudaMemcpy2D(x->d_base, row_bytes, rows, (size_t)dim * 4, (size_t)dim * 4, (size_t)n,
@@ -561,14 +568,16 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
     t.alloc_ms = ms(t0, t1);
     cudaStream_t st = x->stream;
     SONG_CUDA(cudaMemsetAsync(x->d_err, 0, sizeof(int), st), "error reset");
+    *x->h_err = 0;
+    // Per batch: copy in, search, copy out, on the index's stream with one
+    // synchronisation at the end of the batch; the copy and kernel times come
+    // from events between them.
     for (int off = 0; off < nq; off += chunk) {
         const int bs = std::min(chunk, nq - off);
-        auto b0 = clk::now();
+        SONG_CUDA(cudaEventRecord(x->ev_h, st), "event");
         SONG_CUDA(cudaMemcpyAsync(x->d_q, (const char*)queries + (size_t)off * qrow, (size_t)bs * qrow,
                                   cudaMemcpyHostToDevice, st),
                   "query H2D");
-        SONG_CUDA(cudaStreamSynchronize(st), "query H2D sync");
-        auto b1 = clk::now();
         song::SearchArgs a;
         if (song_status s = make_args(x, x->d_q, bs, k, ef, x->d_ids, traces ? x->d_tr : nullptr, &a,
                                       opts, dists ? x->d_dist : nullptr))
@@ -576,10 +585,6 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
         SONG_CUDA(cudaEventRecord(x->ev0, st), "event");
         if (song_status s = launch(x, a, st)) return s;
         SONG_CUDA(cudaEventRecord(x->ev1, st), "event");
-        SONG_CUDA(cudaStreamSynchronize(st), "search kernel");
-        float kms = 0.f;
-        cudaEventElapsedTime(&kms, x->ev0, x->ev1);
-        auto b2 = clk::now();
         if (k > 0)
             SONG_CUDA(cudaMemcpyAsync(ids + (size_t)off * k, x->d_ids, (size_t)bs * k * 4,
                                       cudaMemcpyDeviceToHost, st),
@@ -592,16 +597,25 @@ song_status host_search(song_index* x, int kind, const void* queries, int nq, in
             SONG_CUDA(cudaMemcpyAsync(dists + (size_t)off * k, x->d_dist, (size_t)bs * k * 4,
                                       cudaMemcpyDeviceToHost, st),
                       "distance D2H");
-        SONG_CUDA(cudaStreamSynchronize(st), "D2H sync");
-        auto b3 = clk::now();
-        t.h2d_ms += ms(b0, b1);
+        if (off + bs >= nq)
+            SONG_CUDA(cudaMemcpyAsync(x->h_err, x->d_err, sizeof(int), cudaMemcpyDeviceToHost, st),
+                      "error flag");
+        SONG_CUDA(cudaEventRecord(x->ev_d, st), "event");
+        SONG_CUDA(cudaStreamSynchronize(st), "search");
+        float hms = 0.f, kms = 0.f, dms = 0.f;
+        cudaEventElapsedTime(&hms, x->ev_h, x->ev0);
+        cudaEventElapsedTime(&kms, x->ev0, x->ev1);
+        cudaEventElapsedTime(&dms, x->ev1, x->ev_d);
+        t.h2d_ms += hms;
         t.kernel_ms += kms;
-        t.d2h_ms += ms(b2, b3);
+        t.d2h_ms += dms;
         t.n_batches += 1;
     }
-    int err = 0;
-    SONG_CUDA(cudaMemcpyAsync(&err, x->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error flag");
-    SONG_CUDA(cudaStreamSynchronize(st), "error flag");
+    if (nq <= 0) {
+        SONG_CUDA(cudaMemcpyAsync(x->h_err, x->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error flag");
+        SONG_CUDA(cudaStreamSynchronize(st), "error flag");
+    }
+    const int err = *x->h_err;
     if (err == 2) return fail(SONG_ERR_TIMEOUT, "the entry stage's bounded wait gave up");
     if (err) return fail(SONG_ERR_INVALID_ARG, "graph holds an out-of-range neighbour id");
     t.total_ms = ms(t1, clk::now());

@@ -76,12 +76,12 @@ typedef struct song_query_trace {
 
 /* The scalar part of GpuSearchTrace (telemetry.h:30-41). Times in ms. */
 typedef struct song_timing {
-    double alloc_ms;
-    double h2d_ms;
+    double alloc_ms;      /* host time of staging-buffer growth */
+    double h2d_ms;        /* CUDA-event time of the query copies */
     double memset_ms;
     double kernel_ms;     /* CUDA-event time of the search kernels */
-    double d2h_ms;
-    double total_ms;
+    double d2h_ms;        /* CUDA-event time of the result copies */
+    double total_ms;      /* host time of the call after allocation */
     int ef_search;        /* ef after the reference clamp */
     int batch_limit;      /* n_multiquery as passed */
     int n_batches;
