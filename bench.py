@@ -661,15 +661,16 @@ def measure_learned(c, details, plain):
     nostop_pts = [p for p in lcurve if p["threshold"] >= 1.0 and p["entry"] == song.ENTRY_MODEL]
     log(f"[rank {c.rank}] learned operating point {op}")
 
-    def opts_of(p, entry=None):
-        return song.SearchOpts(precision=prec, learned=True, stop_threshold=p["threshold"],
-                               beam=p["beam"], bloom_hashes=p["bloom_hashes"],
+    def opts_of(p, entry=None, precision=None):
+        return song.SearchOpts(precision=prec if precision is None else precision, learned=True,
+                               stop_threshold=p["threshold"], beam=p["beam"],
+                               bloom_hashes=p["bloom_hashes"],
                                entry=p["entry"] if entry is None else entry)
 
-    def evaluate(p, entry=None, reps_=5):
+    def evaluate(p, entry=None, reps_=5, precision=None):
         """Recall, QPS and trace means of point p on the evaluation queries."""
         song.set_model(g, blobs[p["trained_ef"]])
-        o = opts_of(p, entry)
+        o = opts_of(p, entry, precision)
         song.search_device_ex(g, o, c.dq, NQ, K, p["ef"], ids_ev, None, c.d_tr[:NQ], stream=stream)
         stream.synchronize()
         rec = float(ds.recall_at_k(ids_ev.cpu().numpy(), c.gt, K).mean())
@@ -717,6 +718,13 @@ def measure_learned(c, details, plain):
         es["reached_on_calibration"], en["reached_on_calibration"] = oks, okn
         ablation["stop_model_on"] = es
         ablation["stop_model_off"] = en
+        # the precision form's storage with the learned stop: BF16 rows (exact for
+        # these integer vectors) at the stop model's operating point
+        song.set_precision(g, song.PREC_BF16)
+        eb, _ = evaluate(bs, precision=song.PREC_BF16)
+        eb["reached_on_calibration"] = oks
+        eb["precision"] = "bf16"
+        ablation["bf16_stop_model_on"] = eb
     details["learned_ablation"] = ablation
 
     # the operating point, timed on the evaluation queries
@@ -794,22 +802,27 @@ def summary_learned(l):
         return l
     ab = l.get("ablation", {})
 
-    def short(e):
+    def short(e, stop=False):
         if e is None:
             return None
         e = e.get("at_target", e)
-        return [e["qps"], e["recall_at_10"], e["ef"]]
+        out = [e["qps"], e["recall_at_10"], e["ef"]]
+        if stop:  # the stop threshold and the share of queries the model stopped
+            out += [e["threshold"], e["learned_stop_rate"]]
+        return out
 
     return {"qps": round(l["qps"], 1), "e2e_qps": round(l["e2e_qps"], 1),
             "recall_at_10": l["recall_at_10"], "ef": l["ef"], "beam": l["beam"],
             "bloom_hashes": l["bloom_hashes"], "bf_words": l.get("bf_words"), "stop_threshold": l["threshold"],
             "entry": l["entry"], "learned_stop_rate": l["learned_stop_rate"],
             "mean_expanded": l["mean_expanded"],
+            "ablation_cols": "qps, recall@10, ef[, stop threshold, share stopped by the model]",
             "ablation_qps_recall_ef": {
                 "entry_model": short(ab.get("entry_model")),
                 "nearest_hubs_no_model": short(ab.get("nearest_hubs")),
                 "reference_seeds_no_entry_stage": short(ab.get("reference_seeds")),
-                "stop_model_on": short(ab.get("stop_model_on")),
+                "stop_model_on": short(ab.get("stop_model_on"), True),
+                "bf16_rows_stop_model_on": short(ab.get("bf16_stop_model_on"), True),
                 "stop_model_off": short(ab.get("stop_model_off"))}}
 
 
