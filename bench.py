@@ -210,7 +210,7 @@ def ncu_traffic(ef: int, bf_words: int, form: str = "plain"):
                 c = e.get("config", {})
                 if (c.get("n"), c.get("nq"), c.get("ef"), c.get("bf_words"), c.get("form", "plain")) == \
                         (N_BASE, NQ, ef, bf_words, form):
-                    return e.get("bytes_per_launch_scaled"), "profiles/search_kernel_traffic.json (ncu, 1 pass)"
+                    return e.get("bytes_per_launch_scaled"), "profiles/search_kernel_traffic.json"
         except (OSError, ValueError):
             pass
     return None, None
@@ -418,11 +418,11 @@ def run_ours(args, ws, rank, local):
                 "ef": best["ef"], "bf_words": LEARN_BF_WORDS if use_learned else plain["bf_words"],
                 "bloom_hashes": best.get("bloom_hashes", 4), "beam": best.get("beam", 1),
                 "graph": graph_src,
-                "storage": "u8 byte rows (base is integer 0-255)" if plain["row_bytes"] < DIM * 4
+                "storage": "u8 byte rows (integer base 0-255)" if plain["row_bytes"] < DIM * 4
                            else "fp32 rows",
-                "arithmetic": "exact integer distances (= the reference's FP32 values)",
-                "selection": f"chosen on {NCAL} calibration queries at recall >= "
-                             f"{TARGET_RECALL}+{SELECT_MARGIN}; reported on the evaluation queries",
+                "arithmetic": "exact integer distances (= reference FP32)",
+                "selection": f"knobs chosen on {NCAL} calibration queries (recall >= "
+                             f"{TARGET_RECALL}+{SELECT_MARGIN}), reported on evaluation queries",
                 "l2": "inputs larger than L2 (data 512 MB + adj 128 MB per GPU)",
                 "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
             },
@@ -816,7 +816,7 @@ def summary_learned(l):
             "bloom_hashes": l["bloom_hashes"], "bf_words": l.get("bf_words"), "stop_threshold": l["threshold"],
             "entry": l["entry"], "learned_stop_rate": l["learned_stop_rate"],
             "mean_expanded": l["mean_expanded"],
-            "ablation_cols": "qps, recall@10, ef[, stop threshold, share stopped by the model]",
+            "ablation_cols": "qps,recall,ef[,stop thr,share stopped]",
             "ablation_qps_recall_ef": {
                 "entry_model": short(ab.get("entry_model")),
                 "nearest_hubs_no_model": short(ab.get("nearest_hubs")),
@@ -1091,7 +1091,8 @@ def measure_c4(c, details):
                      "timing_s": {"generate": round(gen_s, 1), "gpu_build": round(build_s, 1),
                                   "learn": round(learn_s, 1)}}
     return {"n": n, "cols": "ef,qps,recall@k",
-            **{k2: [v.get("ef"), v.get("qps"), v.get("recall")] for k2, v in out.items()}}
+            **{k2: [v.get("ef"), v.get("qps"), v.get("recall")] for k2, v in out.items()
+               if v.get("qps") is not None}}
 
 
 def measure_c4h(c, details):
@@ -1144,8 +1145,8 @@ def cpu_baseline(base, adj, queries, gt, ef, sample=3000):
     cg.close()
     return {"value": round(sample / dt, 1), "unit": "queries/s", "cores": threads,
             "kind": "reference",
-            "sample": f"{sample} eval queries at ef={ef}, Graph::search (graph.h:33) "
-                      f"from oracle/_ref on {threads} threads; its recall@10 {rec:.4f}"}
+            "sample": f"{sample} eval queries, ef={ef}, Graph::search (graph.h:33), "
+                      f"oracle/_ref, {threads} threads; recall@10 {rec:.4f}"}
 
 
 def reference_gpu(base, adj, queries, ef, bf_words, ours):
