@@ -516,9 +516,12 @@ __device__ __forceinline__ unsigned bloom_chunk(uint64_t* bloom, int nb, const B
             if (h < bc.nhash) {
                 const uint32_t p = bf_pos(h, (uint32_t)nb, bc);
                 pos[h] = p;
-                wd[h] = bc.shift >= 0 ? (p & bc.wmask) : (p % bc.words);
-                bt[h] = bc.shift >= 0 ? (p >> bc.shift) : (p / bc.words);
-                if (!((bloom[wd[h]] >> bt[h]) & 1ull)) unc |= 1u << h;
+                const uint32_t w64 = bc.shift >= 0 ? (p & bc.wmask) : (p % bc.words);
+                const uint32_t b64 = bc.shift >= 0 ? (p >> bc.shift) : (p / bc.words);
+                // the same bit as a 32-bit word: the low half of 64-bit word w is word 2w
+                wd[h] = 2u * w64 + (b64 >> 5);
+                bt[h] = b64 & 31u;
+                if (!((reinterpret_cast<const uint32_t*>(bloom)[wd[h]] >> bt[h]) & 1u)) unc |= 1u << h;
             }
         }
     }
@@ -528,9 +531,8 @@ __device__ __forceinline__ unsigned bloom_chunk(uint64_t* bloom, int nb, const B
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
             if ((unc >> h) & 1u) {
-                const unsigned long long old =
-                    atomicOr((unsigned long long*)&bloom[wd[h]], 1ull << bt[h]);
-                if ((old >> bt[h]) & 1ull) event = true;
+                const unsigned old = atomicOr(reinterpret_cast<unsigned*>(bloom) + wd[h], 1u << bt[h]);
+                if ((old >> bt[h]) & 1u) event = true;
             }
         }
     }

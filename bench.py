@@ -302,17 +302,18 @@ def timed_host(torch, dist, ws, dev, steps, warmup, call):
 
 
 def launch_ms(torch, stream, fn, reps=3):
-    """Median CUDA-event time of `reps` launches of fn (one untimed first)."""
+    """CUDA-event time per launch of `reps` launches of fn issued back to back
+    (one untimed first): the same overlap of consecutive launches as the timed
+    region, so the calibration ranks points by what is then reported."""
     fn()
-    out = []
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     for _ in range(reps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
         fn()
-        e1.record(stream)
-        stream.synchronize()
-        out.append(e0.elapsed_time(e1))
-    return statistics.median(out)
+    e1.record(stream)
+    stream.synchronize()
+    return e0.elapsed_time(e1) / reps
 
 
 # ------------------------------------------------------------------ our arm
@@ -573,7 +574,7 @@ def measure_queue_sweep(c, details, bf_words):
     for ef in EF_SWEEP_K100:
         ids_v = c.d_ids100[:NCAL]
         ms = launch_ms(torch, stream, lambda: song.search_device(g, c.dcal, NCAL, 100, ef, ids_v, None,
-                                                                 stream=stream), reps=1)
+                                                                 stream=stream), reps=3)
         rec = float(ds.recall_at_k(ids_v.cpu().numpy(), gt_cal100, 100).mean())
         cal_pts.append({"ef": ef, "recall_cal": round(rec, 4), "qps": round(NCAL / ms * 1e3)})
         if rec >= TARGET_RECALL + SELECT_MARGIN:
@@ -695,7 +696,7 @@ def measure_learned(c, details, plain):
             stream.synchronize()
             rec = float(ds.recall_at_k(ids_cal.cpu().numpy(), c.gt_cal, K).mean())
             ms = launch_ms(torch, stream, lambda: song.search_device_ex(
-                g, o, c.dcal, NCAL, K, ef, ids_cal, None, None, stream=stream), reps=1)
+                g, o, c.dcal, NCAL, K, ef, ids_cal, None, None, stream=stream), reps=3)
             pts.append(dict(p, recall_cal=round(rec, 4), qps=round(NCAL / ms * 1e3)))
             if rec >= TARGET_RECALL + SELECT_MARGIN:
                 break
